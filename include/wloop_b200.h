@@ -1,0 +1,138 @@
+/*
+ * wloop_b200.h -- C ABI of the B200 (sm_100a) implementation of the wloop
+ * measurement path: HYP smearing, APE / spatial-HYP smearing of the spatial
+ * links, temporal and spatial line products and the time-slice resolved
+ * Wilson-loop correlation matrices W(sl1,sl2;t,r;x0).
+ *
+ * All entry points take plain pointers and sizes.  Functions return 0 on
+ * success and -1 on failure; wlg_last_error() then describes the failure
+ * (CUDA errors name the kernel).  No entry point falls back to the CPU: with
+ * no usable GPU every compute call fails.
+ *
+ * Host field layout ("AoS lexicographic"): link (s,mu) of site
+ * s = x3 + N3*(x2 + N2*(x1 + N1*x0)) is the su3_dble at aos + 18*(4*s+mu),
+ * i.e. 9 (re,im) pairs c11..c33.  The openQCD layout of udfld()/alloc_lnk()
+ * (8 links per odd point, modules/lnk/lnkcom.c:840-859) is accepted through
+ * wlg_upload_openqcd() with the caller's ipt[] table.
+ *
+ * Boundary conditions: bc = 0 open (temporal links at x0=N0-1 are zero, as
+ * openQCD's set_bc() leaves them), bc = 3 periodic.
+ *
+ * Precision: WLG_FP64 keeps links and staples in FP64 (the reference form).
+ * WLG_MIXED stores links and computes staples / line products in FP32 and
+ * keeps the SU(3) projection and all loop and plaquette sums in FP64.
+ */
+#ifndef WLOOP_B200_H
+#define WLOOP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Raised from the reference's MAX_SM_LEVELS (5, include/wloop.h:13) so that
+ * six-level runs fit. */
+#define WLG_MAX_SM_LEVELS 8
+
+#define WLG_FP64 0
+#define WLG_MIXED 1
+
+#define WLG_OP_APE 0 /* op_smear_t APE, include/wloop.h:17-21 */
+#define WLG_OP_HYP 1 /* op_smear_t HYP */
+
+/* Mirrors wloop_parms_t (include/wloop.h:24-36) without the result pointer. */
+typedef struct {
+  int msl;                     /* number of smearing levels */
+  int nss[WLG_MAX_SM_LEVELS];  /* sweeps added per level (incremental, smear.c:109-120) */
+  int mwlt;                    /* maximal temporal extent, 1 <= mwlt <= N0/2+1 */
+  int mwlr;                    /* maximal spatial extent,  1 <= mwlr <= Nk/2+1 */
+  int op_smear;                /* WLG_OP_APE or WLG_OP_HYP */
+  double alpha_action[3];      /* HYP parameters for the static action */
+  double alpha_ape;            /* APE parameter for the spatial links */
+  double alpha_hyp[2];         /* spatial HYP parameters */
+  int proj_iter;               /* projection iterations; projection on iff > 0 */
+} wlg_wloop_parms;
+
+typedef struct wlg_ctx wlg_ctx;
+
+/* ---- errors and devices ------------------------------------------------ */
+const char* wlg_last_error(void);
+int wlg_device_count(void);
+int wlg_version(void);
+
+/* ---- context: one lattice resident on one GPU ---------------------------
+ * Replaces the module-static state of hyp_links.c, ape_links.c, smear.c and
+ * wloop.c (all file-static there, e.g. hyp_links.c:68-73, wloop.c:62-67). */
+int wlg_create(const int n[4], int bc, int precision, int device, wlg_ctx** out);
+int wlg_destroy(wlg_ctx* ctx);
+int wlg_sync(wlg_ctx* ctx);
+/* Frees smearing and loop scratch (free_hyp, free_ape_links, free_smear,
+ * free_wloop); the gauge field stays. */
+int wlg_free_scratch(wlg_ctx* ctx);
+
+/* ---- gauge field transfers ---------------------------------------------- */
+int wlg_upload_links(wlg_ctx* ctx, const double* aos);
+int wlg_download_links(wlg_ctx* ctx, double* aos);
+int wlg_upload_openqcd(wlg_ctx* ctx, const double* ud, const int* ipt);
+int wlg_download_openqcd(wlg_ctx* ctx, double* ud, const int* ipt);
+/* Synthetic field on the device (same bytes as wlg_generate_links). */
+int wlg_generate(wlg_ctx* ctx, uint64_t seed, double eps);
+/* Synthetic field on the host into aos (4*V links).  Link (s,mu) is
+ * exp(i eps sum_a h_a lambda_a), h_a ~ N(0,1) from Philox4x32-10 keyed by
+ * seed, reunitarised; open bc zeroes the temporal links at x0=N0-1. */
+int wlg_generate_links(const int n[4], int bc, uint64_t seed, double eps, double* aos);
+/* Uniform [0,1) draw used for per-configuration parameters. */
+double wlg_aux_uniform(uint64_t seed, uint64_t index, uint32_t tag);
+
+/* ---- smearing ------------------------------------------------------------
+ * HYP smearing of the links of directions [mu0,mu1) in place
+ * (hyp_links: 0,4; hyp_time_links: 0,1; hyp_space_links: 1,4;
+ *  modules/smear/hyp_links.c:398-472).  Skipped when a1 == 0 (:405). */
+int wlg_hyp(wlg_ctx* ctx, double a1, double a2, double a3, int proj, int piter, int mu0, int mu1,
+            int keep);
+/* nsweeps APE sweeps U <- P[U + alpha * staples] (ape_links.c:217-284);
+ * time = 1 smears all four directions, time = 0 only the spatial ones. */
+int wlg_ape(wlg_ctx* ctx, double alpha, int proj, int piter, int time, int nsweeps, int keep);
+/* nsweeps two-level spatial HYP sweeps (hyp_spatial_links.c:289-344). */
+int wlg_hyp_spatial(wlg_ctx* ctx, double a1, double a2, int proj, int piter, int nsweeps,
+                    int keep);
+/* Sum of Re tr U(p) over all plaquettes (lnk_plaq_sum, lnkplaq.c:117-128). */
+int wlg_plaq_sum(wlg_ctx* ctx, double* out);
+
+/* ---- Wilson loops ----------------------------------------------------------
+ * wloop_sum on the current (HYP-smeared) field: spatial smearing levels
+ * (smear.c:99-121), then for r,t all msl x msl loops per time slice
+ * (wloop.c:524-608).  wl_mat receives msl*msl*mwlt*mwlr*N0 doubles at
+ * wl_idx(sl1,sl2,t,r,x0) = sl1+msl*(sl2+msl*(t+mwlt*(r+mwlr*x0)))
+ * (wloop_parms.c:431-434).  plaq (optional, msl doubles) receives the
+ * plaquette sum after each level. */
+int wlg_wloop_sum(wlg_ctx* ctx, const wlg_wloop_parms* p, double* wl_mat, double* plaq);
+/* HYP (alpha_action, all directions, as ms10 set_data does: main/ms10.c:633-646)
+ * followed by wlg_wloop_sum. */
+int wlg_measure(wlg_ctx* ctx, const wlg_wloop_parms* p, double* wl_mat, double* plaq);
+/* Level store after wlg_wloop_sum: spatial links of level sl in AoS
+ * [V][3][18] (get_pus, smear.c:124-127). */
+int wlg_download_level(wlg_ctx* ctx, int sl, double* aos3);
+
+/* ---- single-field kernels of the lnk/smear API ------------------------------
+ * vb(x,mu) += staples of the (mu,nu) plane, nu-links from u1, mu-links from
+ * u2 (staple_sum, staple_sum.c:53-87); fields in AoS lexicographic layout. */
+int wlg_staple_sum(const int n[4], const double* u1, const double* u2, int mu, int nu, double* vb);
+/* In-place projection of nmat packed su3_dble matrices
+ * (approx_project_to_su3_dble, projection.c:120-154). */
+int wlg_project(double* mats, int nmat, int iter);
+
+/* ---- kernel timing (CUDA events on the context's stream) ------------------ */
+int wlg_set_profiling(wlg_ctx* ctx, int on);
+/* name: "hyp", "ape", "plaq", "lines", "contract", "reduce" */
+int wlg_kernel_time(wlg_ctx* ctx, const char* name, double* total_ms, long long* launches);
+int wlg_reset_kernel_times(wlg_ctx* ctx);
+/* Tuning knobs of the contraction kernel (0 = automatic). */
+int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

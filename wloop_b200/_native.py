@@ -1,0 +1,98 @@
+"""ctypes binding of libwloop_b200.so (the C ABI in include/wloop_b200.h).
+
+The library is built in-tree by ``python -m wloop_b200.build``.  Importing
+this module without the built library raises: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libwloop_b200.so")
+
+WLG_MAX_SM_LEVELS = 8
+WLG_FP64 = 0
+WLG_MIXED = 1
+WLG_OP_APE = 0
+WLG_OP_HYP = 1
+
+
+class WlgParms(C.Structure):
+    """Mirror of wlg_wloop_parms (include/wloop_b200.h)."""
+    _fields_ = [
+        ("msl", C.c_int),
+        ("nss", C.c_int * WLG_MAX_SM_LEVELS),
+        ("mwlt", C.c_int),
+        ("mwlr", C.c_int),
+        ("op_smear", C.c_int),
+        ("alpha_action", C.c_double * 3),
+        ("alpha_ape", C.c_double),
+        ("alpha_hyp", C.c_double * 2),
+        ("proj_iter", C.c_int),
+    ]
+
+
+class WlgError(RuntimeError):
+    pass
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"wloop_b200: native library {LIB_PATH} is not built; run "
+            "`python -m wloop_b200.build` (the CUDA path has no CPU fallback)")
+    lib = C.CDLL(LIB_PATH, mode=C.RTLD_GLOBAL)
+    vp, ip, dp, i, d = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int, C.c_double
+    u64, u32 = C.c_uint64, C.c_uint32
+    sig = {
+        "wlg_last_error": (C.c_char_p, []),
+        "wlg_device_count": (i, []),
+        "wlg_version": (i, []),
+        "wlg_create": (i, [ip, i, i, i, C.POINTER(vp)]),
+        "wlg_destroy": (i, [vp]),
+        "wlg_sync": (i, [vp]),
+        "wlg_free_scratch": (i, [vp]),
+        "wlg_upload_links": (i, [vp, dp]),
+        "wlg_download_links": (i, [vp, dp]),
+        "wlg_upload_openqcd": (i, [vp, dp, ip]),
+        "wlg_download_openqcd": (i, [vp, dp, ip]),
+        "wlg_generate": (i, [vp, u64, d]),
+        "wlg_generate_links": (i, [ip, i, u64, d, dp]),
+        "wlg_aux_uniform": (d, [u64, u64, u32]),
+        "wlg_hyp": (i, [vp, d, d, d, i, i, i, i, i]),
+        "wlg_ape": (i, [vp, d, i, i, i, i, i]),
+        "wlg_hyp_spatial": (i, [vp, d, d, i, i, i, i]),
+        "wlg_plaq_sum": (i, [vp, dp]),
+        "wlg_wloop_sum": (i, [vp, C.POINTER(WlgParms), dp, dp]),
+        "wlg_measure": (i, [vp, C.POINTER(WlgParms), dp, dp]),
+        "wlg_download_level": (i, [vp, i, dp]),
+        "wlg_staple_sum": (i, [ip, dp, dp, i, i, dp]),
+        "wlg_project": (i, [dp, i, i]),
+        "wlg_set_profiling": (i, [vp, i]),
+        "wlg_kernel_time": (i, [vp, C.c_char_p, dp, C.POINTER(C.c_longlong)]),
+        "wlg_reset_kernel_times": (i, [vp]),
+        "wlg_set_contract_shape": (i, [vp, i, i, i]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != 0:
+        msg = lib.wlg_last_error().decode(errors="replace")
+        raise WlgError(f"{what}: {msg}" if what else msg)
+
+
+def dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def iptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))

@@ -1,0 +1,276 @@
+// common.cuh -- device types shared by every wloop_b200 kernel.
+//
+// Link fields live in HBM as structure-of-arrays: for direction mu, complex
+// component c (row-major c11..c33 -> 0..8) and lexicographic site s
+//     field[(mu*9 + c)*vol + s]          (double2 in FP64, float2 in mixed)
+// so a warp reading component c of 32 consecutive sites issues one fully
+// coalesced 512 B (FP64) or 256 B (FP32) request.  The site index is
+// s = x3 + N3*(x2 + N2*(x1 + N1*x0)), the argument order of openQCD's ipt[].
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define WLG_MAX_LEVELS 8
+
+namespace wlg {
+
+template <class T> struct V2;
+template <> struct V2<double> { typedef double2 t; };
+template <> struct V2<float> { typedef float2 t; };
+
+// A 3x3 complex matrix held in registers, row-major.
+template <class T> struct M3 {
+  typename V2<T>::t e[9];
+};
+
+// ---------------------------------------------------------------------------
+// Geometry
+// ---------------------------------------------------------------------------
+struct Geo {
+  int n[4];    // N0 (time), N1, N2, N3
+  int st[4];   // strides: st[0]=N1*N2*N3, st[1]=N2*N3, st[2]=N3, st[3]=1
+  int vol;     // N0*N1*N2*N3
+  int vs;      // N1*N2*N3 (one time slice)
+};
+
+static inline Geo make_geo(const int n[4]) {
+  Geo g;
+  for (int i = 0; i < 4; i++) g.n[i] = n[i];
+  g.st[3] = 1;
+  g.st[2] = n[3];
+  g.st[1] = n[2] * n[3];
+  g.st[0] = n[1] * n[2] * n[3];
+  g.vs = g.st[0];
+  g.vol = n[0] * g.st[0];
+  return g;
+}
+
+__device__ __forceinline__ void coords(const Geo& g, int s, int x[4]) {
+  x[0] = s / g.st[0];
+  int r = s - x[0] * g.st[0];
+  x[1] = r / g.st[1];
+  r -= x[1] * g.st[1];
+  x[2] = r / g.st[2];
+  x[3] = r - x[2] * g.st[2];
+}
+
+// neighbour of site s (coordinate xm along mu) shifted by +1 / -1, periodic
+__device__ __forceinline__ int up(const Geo& g, int s, int xm, int mu) {
+  return (xm == g.n[mu] - 1) ? s - (g.n[mu] - 1) * g.st[mu] : s + g.st[mu];
+}
+__device__ __forceinline__ int dn(const Geo& g, int s, int xm, int mu) {
+  return (xm == 0) ? s + (g.n[mu] - 1) * g.st[mu] : s - g.st[mu];
+}
+// shift by +d (0 <= d < N_mu), periodic
+__device__ __forceinline__ int shift(const Geo& g, int s, int xm, int mu, int d) {
+  int y = xm + d;
+  if (y >= g.n[mu]) y -= g.n[mu];
+  return s + (y - xm) * g.st[mu];
+}
+
+// ---------------------------------------------------------------------------
+// Field views: one base pointer per direction (any may be null when a kernel
+// never touches that direction).  Component c of link (s,mu) is at
+// p[mu][c*vol + s].
+// ---------------------------------------------------------------------------
+template <class T> struct Links {
+  typename V2<T>::t* p[4];
+};
+
+template <class T>
+__device__ __forceinline__ void ld(M3<T>& m, const typename V2<T>::t* __restrict__ base, int vol,
+                                   int s) {
+#pragma unroll
+  for (int c = 0; c < 9; c++) m.e[c] = __ldg(base + (size_t)c * vol + s);
+}
+
+template <class T>
+__device__ __forceinline__ void st(typename V2<T>::t* __restrict__ base, int vol, int s,
+                                   const M3<T>& m) {
+#pragma unroll
+  for (int c = 0; c < 9; c++) base[(size_t)c * vol + s] = m.e[c];
+}
+
+// ---------------------------------------------------------------------------
+// SU(3) algebra (definitions of openQCD's su3xsu3, su3dagxsu3, su3xsu3dag).
+// ---------------------------------------------------------------------------
+template <class T> __device__ __forceinline__ void zero(M3<T>& a) {
+#pragma unroll
+  for (int c = 0; c < 9; c++) {
+    a.e[c].x = T(0);
+    a.e[c].y = T(0);
+  }
+}
+
+// c = a*b
+template <class T> __device__ __forceinline__ void mul(M3<T>& c, const M3<T>& a, const M3<T>& b) {
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      T re = a.e[3 * i].x * b.e[j].x - a.e[3 * i].y * b.e[j].y;
+      T im = a.e[3 * i].x * b.e[j].y + a.e[3 * i].y * b.e[j].x;
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        re = fma(a.e[3 * i + k].x, b.e[3 * k + j].x, re);
+        re = fma(-a.e[3 * i + k].y, b.e[3 * k + j].y, re);
+        im = fma(a.e[3 * i + k].x, b.e[3 * k + j].y, im);
+        im = fma(a.e[3 * i + k].y, b.e[3 * k + j].x, im);
+      }
+      c.e[3 * i + j].x = re;
+      c.e[3 * i + j].y = im;
+    }
+}
+
+// c = a^dag * b
+template <class T> __device__ __forceinline__ void mul_da(M3<T>& c, const M3<T>& a, const M3<T>& b) {
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      T re = a.e[i].x * b.e[j].x + a.e[i].y * b.e[j].y;
+      T im = a.e[i].x * b.e[j].y - a.e[i].y * b.e[j].x;
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        re = fma(a.e[3 * k + i].x, b.e[3 * k + j].x, re);
+        re = fma(a.e[3 * k + i].y, b.e[3 * k + j].y, re);
+        im = fma(a.e[3 * k + i].x, b.e[3 * k + j].y, im);
+        im = fma(-a.e[3 * k + i].y, b.e[3 * k + j].x, im);
+      }
+      c.e[3 * i + j].x = re;
+      c.e[3 * i + j].y = im;
+    }
+}
+
+// c = a * b^dag
+template <class T> __device__ __forceinline__ void mul_ad(M3<T>& c, const M3<T>& a, const M3<T>& b) {
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      T re = a.e[3 * i].x * b.e[3 * j].x + a.e[3 * i].y * b.e[3 * j].y;
+      T im = a.e[3 * i].y * b.e[3 * j].x - a.e[3 * i].x * b.e[3 * j].y;
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        re = fma(a.e[3 * i + k].x, b.e[3 * j + k].x, re);
+        re = fma(a.e[3 * i + k].y, b.e[3 * j + k].y, re);
+        im = fma(a.e[3 * i + k].y, b.e[3 * j + k].x, im);
+        im = fma(-a.e[3 * i + k].x, b.e[3 * j + k].y, im);
+      }
+      c.e[3 * i + j].x = re;
+      c.e[3 * i + j].y = im;
+    }
+}
+
+template <class T> __device__ __forceinline__ void acc(M3<T>& c, const M3<T>& a) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    c.e[k].x += a.e[k].x;
+    c.e[k].y += a.e[k].y;
+  }
+}
+
+// Re tr(a^dag b) = sum_ij Re(conj(a_ij) b_ij)  (openQCD _vector_prod_re over rows)
+template <class T> __device__ __forceinline__ T retr_dag(const M3<T>& a, const M3<T>& b) {
+  T s = a.e[0].x * b.e[0].x;
+  s = fma(a.e[0].y, b.e[0].y, s);
+#pragma unroll
+  for (int k = 1; k < 9; k++) {
+    s = fma(a.e[k].x, b.e[k].x, s);
+    s = fma(a.e[k].y, b.e[k].y, s);
+  }
+  return s;
+}
+
+template <class D, class S> __device__ __forceinline__ void cvt(M3<D>& d, const M3<S>& s) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    d.e[k].x = (D)s.e[k].x;
+    d.e[k].y = (D)s.e[k].y;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Approximate SU(3) projection of hep-lat/0506008 as implemented by
+// approx_project_to_su3_dble (modules/smear/projection.c:120-154).  Always FP64.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double det_im(const M3<double>& u) {
+  const double2* c = u.e;
+  double d1re = (c[4].x * c[8].x - c[4].y * c[8].y) - (c[5].x * c[7].x - c[5].y * c[7].y);
+  double d1im = (c[4].x * c[8].y + c[4].y * c[8].x) - (c[5].x * c[7].y + c[5].y * c[7].x);
+  double d2re = (c[3].x * c[8].x - c[3].y * c[8].y) - (c[5].x * c[6].x - c[5].y * c[6].y);
+  double d2im = (c[3].x * c[8].y + c[3].y * c[8].x) - (c[5].x * c[6].y + c[5].y * c[6].x);
+  double d3re = (c[3].x * c[7].x - c[3].y * c[7].y) - (c[4].x * c[6].x - c[4].y * c[6].y);
+  double d3im = (c[3].x * c[7].y + c[3].y * c[7].x) - (c[4].x * c[6].y + c[4].y * c[6].x);
+  return (c[0].x * d1im + c[0].y * d1re) - (c[1].x * d2im + c[1].y * d2re) +
+         (c[2].x * d3im + c[2].y * d3re);
+}
+
+#define WLG_SRT18_EPS (4.242640687119285 * 2.220446049250313080847e-16)
+
+__device__ __forceinline__ void project(M3<double>& u, int iter) {
+  double d = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; k++) d += u.e[k].x * u.e[k].x + u.e[k].y * u.e[k].y;
+  if (d < WLG_SRT18_EPS) return;  // zero guard, projection.c:136
+  d = 1.0 / sqrt(d / 3.0);
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    u.e[k].x *= d;
+    u.e[k].y *= d;
+  }
+  for (int it = 0; it < iter; it++) {
+    M3<double> x, y;
+    mul_da(x, u, u);
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      x.e[k].x *= -0.5;
+      x.e[k].y *= -0.5;
+    }
+    x.e[0].x += 1.5;
+    x.e[4].x += 1.5;
+    x.e[8].x += 1.5;
+    mul(y, u, x);
+    double zim = det_im(y) / -3.0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      u.e[k].x = y.e[k].x - zim * y.e[k].y;
+      u.e[k].y = y.e[k].y + zim * y.e[k].x;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Up and down staples of link (x,mu) in the (mu,nu) plane, general 3x3 form
+// (add_up_staple_save / add_dn_staple_save, modules/lnk/lnkstaple.c:318-382):
+//   up = u1(x,nu) u2(x+nu,mu) u1(x+mu,nu)^dag
+//   dn = u1(x-nu,nu)^dag u2(x-nu,mu) u1(x-nu+mu,nu)
+// nu-links come from a, mu-links from b; the sum is added to v.
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ void add_staples(M3<T>& v, const Geo& g, const int x[4], int s,
+                                            const typename V2<T>::t* __restrict__ a_nu,
+                                            const typename V2<T>::t* __restrict__ b_mu, int mu,
+                                            int nu) {
+  const int vol = g.vol;
+  M3<T> p, q, r;
+  int s_pn = up(g, s, x[nu], nu);
+  int s_pm = up(g, s, x[mu], mu);
+  ld(p, b_mu, vol, s_pn);
+  ld(q, a_nu, vol, s_pm);
+  mul_ad(r, p, q);
+  ld(p, a_nu, vol, s);
+  mul(q, p, r);
+  acc(v, q);
+  int s_mn = dn(g, s, x[nu], nu);
+  int xm = x[mu];  // x-nu has the same mu coordinate
+  int s_mn_pm = up(g, s_mn, xm, mu);
+  ld(p, b_mu, vol, s_mn);
+  ld(q, a_nu, vol, s_mn_pm);
+  mul(r, p, q);
+  ld(p, a_nu, vol, s_mn);
+  mul_da(q, p, r);
+  acc(v, q);
+}
+
+}  // namespace wlg

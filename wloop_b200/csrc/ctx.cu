@@ -1,0 +1,709 @@
+// ctx.cu -- the C ABI (include/wloop_b200.h): a context owns one lattice on
+// one GPU, its scratch buffers and its stream, and sequences the kernels of
+// smear.cu / loops.cu / layout.cu.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+#include <map>
+#include <string>
+#include <vector>
+#include "internal.h"
+#include "../../include/wloop_b200.h"
+
+namespace wlg {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+const char* get_error() { return g_err; }
+
+int num_sms() {
+  static int cached[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (cached[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+    cached[dev] = n;
+  }
+  return cached[dev];
+}
+
+}  // namespace wlg
+
+using namespace wlg;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct ProfStat {
+  double ms = 0.0;
+  long long n = 0;
+};
+
+struct wlg_ctx {
+  int dev = 0, prec = WLG_FP64, bc = 3;
+  Geo g;
+  cudaStream_t st = nullptr;
+  DevBuf U, bar, til, apeA, apeB, dl, levels, lines, partial, wl, plaq_part, plaq_out, staging, ipt;
+  int cG = 0, cNCB = 0, cBlock = 0;
+  bool prof = false;
+  std::map<std::string, ProfStat> stats;
+  struct Pending {
+    std::string name;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> evpool;
+  int last_msl = 0;
+};
+
+static int ensure(DevBuf& b, size_t bytes) {
+  if (b.cap >= bytes && b.p) return 0;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  if (bytes == 0) return 0;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+    cudaGetLastError();
+    return -1;
+  }
+  b.cap = bytes;
+  return 0;
+}
+
+static void release(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+static size_t link_bytes(const wlg_ctx* c) { return c->prec == WLG_FP64 ? 16 * 9 : 8 * 9; }
+static size_t field_bytes(const wlg_ctx* c, int ndir) {
+  return (size_t)ndir * link_bytes(c) * (size_t)c->g.vol;
+}
+
+template <class T> static Links<T> view4(void* base, int vol) {
+  Links<T> L;
+  typename V2<T>::t* b = (typename V2<T>::t*)base;
+  for (int mu = 0; mu < 4; mu++) L.p[mu] = b ? b + (size_t)mu * 9 * vol : nullptr;
+  return L;
+}
+// spatial-only field stored as 3 directions: p[0] is null
+template <class T> static Links<T> view3(void* base, int vol) {
+  Links<T> L;
+  typename V2<T>::t* b = (typename V2<T>::t*)base;
+  L.p[0] = nullptr;
+  for (int k = 1; k < 4; k++) L.p[k] = b + (size_t)(k - 1) * 9 * vol;
+  return L;
+}
+
+static cudaEvent_t get_event(wlg_ctx* c) {
+  if (!c->evpool.empty()) {
+    cudaEvent_t e = c->evpool.back();
+    c->evpool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct ProfScope {
+  wlg_ctx* c;
+  const char* name;
+  cudaEvent_t a = nullptr;
+  ProfScope(wlg_ctx* c_, const char* n) : c(c_), name(n) {
+    if (c->prof) {
+      a = get_event(c);
+      cudaEventRecord(a, c->st);
+    }
+  }
+  ~ProfScope() {
+    if (c->prof) {
+      cudaEvent_t b = get_event(c);
+      cudaEventRecord(b, c->st);
+      c->pending.push_back({name, a, b});
+    }
+  }
+};
+
+static void harvest(wlg_ctx* c) {
+  if (c->pending.empty()) return;
+  cudaStreamSynchronize(c->st);
+  for (auto& p : c->pending) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    ProfStat& s = c->stats[p.name];
+    s.ms += ms;
+    s.n += 1;
+    c->evpool.push_back(p.a);
+    c->evpool.push_back(p.b);
+  }
+  c->pending.clear();
+}
+
+static int finish(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return -1;
+  }
+  if (get_error()[0] && strncmp(get_error(), "kernel ", 7) == 0) return -1;
+  return 0;
+}
+
+#define CTX_BEGIN(c)                                  \
+  do {                                                \
+    if (!(c)) {                                       \
+      set_error("null context");                      \
+      return -1;                                      \
+    }                                                 \
+    set_error("%s", "");                              \
+    WLG_CUDA(cudaSetDevice((c)->dev));                \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// typed implementations
+// ---------------------------------------------------------------------------
+template <class T> static int do_hyp(wlg_ctx* c, double a1, double a2, double a3, int proj,
+                                     int piter, int mu0, int mu1, int keep) {
+  if (a1 == 0.0) return 0;  // hyp_links.c:405
+  size_t fb = field_bytes(c, 12);
+  if (ensure(c->bar, fb) || ensure(c->til, fb)) return -1;
+  Links<T> U = view4<T>(c->U.p, c->g.vol);
+  {
+    ProfScope ps(c, "hyp");
+    hyp_level3<T>(c->g, U, (typename V2<T>::t*)c->bar.p, a3, proj, piter, c->st);
+    hyp_level2<T>(c->g, U, (const typename V2<T>::t*)c->bar.p, (typename V2<T>::t*)c->til.p, a2,
+                  proj, piter, c->st);
+    hyp_level1<T>(c->g, U, (const typename V2<T>::t*)c->til.p, a1, proj, piter, mu0, mu1, c->bc,
+                  c->st);
+  }
+  if (!keep) {
+    WLG_CUDA(cudaStreamSynchronize(c->st));
+    release(c->bar);
+    release(c->til);
+  }
+  return finish("hyp");
+}
+
+template <class T> static int do_ape(wlg_ctx* c, double alpha, int proj, int piter, int time,
+                                     int nsweeps, int keep) {
+  if (nsweeps <= 0) return 0;
+  int mu0 = time ? 0 : 1;
+  if (ensure(c->apeA, field_bytes(c, 4))) return -1;
+  Links<T> U = view4<T>(c->U.p, c->g.vol), A = view4<T>(c->apeA.p, c->g.vol);
+  {
+    ProfScope ps(c, "ape");
+    for (int i = 0; i < nsweeps; i++) {
+      if (i % 2 == 0)
+        ape_sweep<T>(c->g, U, A, alpha, proj, piter, mu0, c->st);
+      else
+        ape_sweep<T>(c->g, A, U, alpha, proj, piter, mu0, c->st);
+    }
+  }
+  if (nsweeps % 2 == 1) {
+    size_t off = (size_t)mu0 * link_bytes(c) * c->g.vol;
+    WLG_CUDA(cudaMemcpyAsync((char*)c->U.p + off, (char*)c->apeA.p + off,
+                             field_bytes(c, 4 - mu0), cudaMemcpyDeviceToDevice, c->st));
+  }
+  if (!keep) {
+    WLG_CUDA(cudaStreamSynchronize(c->st));
+    release(c->apeA);
+  }
+  return finish("ape");
+}
+
+
+// one spatial-HYP sweep src -> dst (dst may equal src)
+template <class T> static int hyp3_sweep(wlg_ctx* c, Links<T> src, Links<T> dst, double a1,
+                                         double a2, int proj, int piter) {
+  if (ensure(c->dl, field_bytes(c, 6))) return -1;
+  hyp3d_level1<T>(c->g, src, (typename V2<T>::t*)c->dl.p, a2, proj, piter, c->st);
+  if (src.p[1] != dst.p[1]) {
+    // level 2 reads only its own src link for the linear combination
+    for (int k = 1; k < 4; k++)
+      WLG_CUDA(cudaMemcpyAsync(dst.p[k], src.p[k], link_bytes(c) * c->g.vol,
+                               cudaMemcpyDeviceToDevice, c->st));
+  }
+  hyp3d_level2<T>(c->g, dst, (const typename V2<T>::t*)c->dl.p, a1, proj, piter, c->st);
+  return 0;
+}
+
+template <class T> static int do_hyp_spatial(wlg_ctx* c, double a1, double a2, int proj, int piter,
+                                             int nsweeps, int keep) {
+  Links<T> U = view4<T>(c->U.p, c->g.vol);
+  {
+    ProfScope ps(c, "hyp3");
+    for (int i = 0; i < nsweeps; i++)
+      if (hyp3_sweep<T>(c, U, U, a1, a2, proj, piter)) return -1;
+  }
+  if (!keep) {
+    WLG_CUDA(cudaStreamSynchronize(c->st));
+    release(c->dl);
+  }
+  return finish("hyp_spatial");
+}
+
+template <class T> static int do_plaq(wlg_ctx* c, Links<T> L, double* dev_out) {
+  if (ensure(c->plaq_part, sizeof(double) * plaq_partials())) return -1;
+  ProfScope ps(c, "plaq");
+  plaq_sum<T>(c->g, c->bc, L, (double*)c->plaq_part.p, dev_out, c->st);
+  return 0;
+}
+
+static int check_parms(const wlg_ctx* c, const wlg_wloop_parms* p) {
+  const int* n = c->g.n;
+  if (!p) {
+    set_error("null parameters");
+    return -1;
+  }
+  if (p->msl < 1 || p->msl > WLG_MAX_SM_LEVELS) {  // wloop_parms.c:156-157
+    set_error("max smearing level out of range (msl=%d)", p->msl);
+    return -1;
+  }
+  if (p->mwlt < 1 || p->mwlt > n[0] / 2 + 1) {  // :174-175
+    set_error("max wloop time extension out of range (mwlt=%d)", p->mwlt);
+    return -1;
+  }
+  if (p->mwlr < 1 || p->mwlr > n[1] / 2 + 1 || p->mwlr > n[2] / 2 + 1 || p->mwlr > n[3] / 2 + 1) {
+    set_error("max wloop spatial extension out of range (mwlr=%d)", p->mwlr);  // :176-177
+    return -1;
+  }
+  if (p->op_smear != WLG_OP_APE && p->op_smear != WLG_OP_HYP) {  // :104-105
+    set_error("Unknown type of operator smearing");
+    return -1;
+  }
+  for (int i = 0; i < p->msl; i++)
+    if (p->nss[i] < 0) {
+      set_error("negative number of smearing steps");
+      return -1;
+    }
+  return 0;
+}
+
+template <class T>
+static int do_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, double* plaq) {
+  if (check_parms(c, p)) return -1;
+  const Geo& g = c->g;
+  const int msl = p->msl, proj = p->proj_iter > 0;
+  const size_t f3 = field_bytes(c, 3);
+  if (ensure(c->levels, f3 * msl) || ensure(c->apeA, f3) || ensure(c->apeB, f3)) return -1;
+  if (ensure(c->plaq_out, sizeof(double) * WLG_MAX_SM_LEVELS)) return -1;
+  c->last_msl = msl;
+  typedef typename V2<T>::t T2;
+  Links<T> U = view4<T>(c->U.p, g.vol);
+  Links<T> A = view3<T>(c->apeA.p, g.vol), B = view3<T>(c->apeB.p, g.vol);
+  auto level = [&](int sl) { return view3<T>((char*)c->levels.p + f3 * sl, g.vol); };
+
+  // ---- smear(): spatial levels (smear.c:99-121) ----
+  Links<T> cur = U;
+  for (int sl = 0; sl < msl; sl++) {
+    Links<T> lv = level(sl);
+    int ns = p->nss[sl];
+    if (ns == 0) {
+      WLG_CUDA(cudaMemcpyAsync(lv.p[1], cur.p[1], link_bytes(c) * g.vol, cudaMemcpyDeviceToDevice, c->st));
+      WLG_CUDA(cudaMemcpyAsync(lv.p[2], cur.p[2], link_bytes(c) * g.vol, cudaMemcpyDeviceToDevice, c->st));
+      WLG_CUDA(cudaMemcpyAsync(lv.p[3], cur.p[3], link_bytes(c) * g.vol, cudaMemcpyDeviceToDevice, c->st));
+    }
+    for (int i = 0; i < ns; i++) {
+      Links<T> dst = (i == ns - 1) ? lv : ((cur.p[1] == A.p[1]) ? B : A);
+      ProfScope ps(c, p->op_smear == WLG_OP_APE ? "ape" : "hyp3");
+      if (p->op_smear == WLG_OP_APE)
+        ape_sweep<T>(g, cur, dst, p->alpha_ape, proj, p->proj_iter, 1, c->st);
+      else if (hyp3_sweep<T>(c, cur, dst, p->alpha_hyp[0], p->alpha_hyp[1], proj, p->proj_iter))
+        return -1;
+      cur = dst;
+    }
+    cur = lv;
+    if (plaq) {
+      Links<T> pl = lv;
+      pl.p[0] = U.p[0];
+      if (do_plaq<T>(c, pl, (double*)c->plaq_out.p + sl)) return -1;
+    }
+  }
+
+  // ---- wloops (wloop.c:524-608) ----
+  ContractPlan cp = contract_plan(g, msl, p->mwlt, c->prec == WLG_FP64, c->cG, c->cNCB, c->cBlock);
+  size_t nwl = (size_t)msl * msl * p->mwlt * p->mwlr * g.n[0];
+  if (ensure(c->partial, sizeof(double) * cp.partial_doubles) || ensure(c->wl, sizeof(double) * nwl))
+    return -1;
+  if (p->mwlr > 1 && ensure(c->lines, f3 * msl)) return -1;
+  const T2* lev = (const T2*)c->levels.p;
+  T2* lines = (T2*)c->lines.p;
+  for (int r = 0; r < p->mwlr; r++) {
+    const int R = r + 1;
+    const T2* L = lev;
+    if (R >= 2) {
+      ProfScope ps(c, "lines");
+      line_step<T>(g, msl, R, lev, R == 2 ? lev : lines, lines, c->st);
+      L = lines;
+    }
+    {
+      ProfScope ps(c, "contract");
+      contract<T>(g, cp, U.p[0], L, msl, p->mwlt, R, (double*)c->partial.p, c->st);
+    }
+    {
+      ProfScope ps(c, "reduce");
+      contract_reduce(g, cp, msl, p->mwlt, p->mwlr, r, (const double*)c->partial.p,
+                      (double*)c->wl.p, c->st);
+    }
+  }
+  if (wl_mat)
+    WLG_CUDA(cudaMemcpyAsync(wl_mat, c->wl.p, sizeof(double) * nwl, cudaMemcpyDeviceToHost, c->st));
+  if (plaq)
+    WLG_CUDA(cudaMemcpyAsync(plaq, c->plaq_out.p, sizeof(double) * msl, cudaMemcpyDeviceToHost, c->st));
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  return finish("wloop_sum");
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* wlg_last_error(void) { return get_error(); }
+
+int wlg_version(void) { return 100; }
+
+int wlg_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int wlg_create(const int n[4], int bc, int precision, int device, wlg_ctx** out) {
+  set_error("%s", "");
+  if (!n || !out) {
+    set_error("null argument");
+    return -1;
+  }
+  for (int i = 0; i < 4; i++)
+    if (n[i] < 2) {
+      set_error("lattice extent N%d=%d < 2", i, n[i]);
+      return -1;
+    }
+  if ((long long)n[0] * n[1] * n[2] * n[3] > (1LL << 30)) {
+    set_error("lattice volume too large");
+    return -1;
+  }
+  if (bc != 0 && bc != 3) {
+    set_error("only open (0) and periodic (3) boundary conditions are supported");
+    return -1;
+  }
+  if (precision != WLG_FP64 && precision != WLG_MIXED) {
+    set_error("unknown precision %d", precision);
+    return -1;
+  }
+  int nd = wlg_device_count();
+  if (nd <= 0) {
+    set_error("no CUDA device available (the wloop_b200 path has no CPU fallback)");
+    return -1;
+  }
+  if (device < 0 || device >= nd) {
+    set_error("device %d out of range (%d devices)", device, nd);
+    return -1;
+  }
+  WLG_CUDA(cudaSetDevice(device));
+  wlg_ctx* c = new wlg_ctx();
+  c->dev = device;
+  c->prec = precision;
+  c->bc = bc;
+  c->g = make_geo(n);
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("cudaStreamCreate failed");
+    delete c;
+    return -1;
+  }
+  if (ensure(c->U, field_bytes(c, 4))) {
+    cudaStreamDestroy(c->st);
+    delete c;
+    return -1;
+  }
+  WLG_CUDA(cudaMemsetAsync(c->U.p, 0, field_bytes(c, 4), c->st));
+  *out = c;
+  return 0;
+}
+
+int wlg_free_scratch(wlg_ctx* c) {
+  CTX_BEGIN(c);
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  release(c->bar);
+  release(c->til);
+  release(c->apeA);
+  release(c->apeB);
+  release(c->dl);
+  release(c->levels);
+  release(c->lines);
+  release(c->partial);
+  release(c->staging);
+  return 0;
+}
+
+int wlg_destroy(wlg_ctx* c) {
+  if (!c) return 0;
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->st);
+  harvest(c);
+  DevBuf* all[] = {&c->U, &c->bar, &c->til, &c->apeA, &c->apeB, &c->dl, &c->levels, &c->lines,
+                   &c->partial, &c->wl, &c->plaq_part, &c->plaq_out, &c->staging, &c->ipt};
+  for (DevBuf* b : all) release(*b);
+  for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
+  cudaStreamDestroy(c->st);
+  delete c;
+  return 0;
+}
+
+int wlg_sync(wlg_ctx* c) {
+  CTX_BEGIN(c);
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  return finish("sync");
+}
+
+int wlg_upload_links(wlg_ctx* c, const double* aos) {
+  CTX_BEGIN(c);
+  size_t bytes = (size_t)4 * 144 * c->g.vol;
+  if (ensure(c->staging, bytes)) return -1;
+  WLG_CUDA(cudaMemcpyAsync(c->staging.p, aos, bytes, cudaMemcpyHostToDevice, c->st));
+  if (c->prec == WLG_FP64)
+    aos_to_soa<double>(c->g, (const double*)c->staging.p, view4<double>(c->U.p, c->g.vol), 0, 4, c->st);
+  else
+    aos_to_soa<float>(c->g, (const double*)c->staging.p, view4<float>(c->U.p, c->g.vol), 0, 4, c->st);
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  return finish("upload_links");
+}
+
+int wlg_download_links(wlg_ctx* c, double* aos) {
+  CTX_BEGIN(c);
+  size_t bytes = (size_t)4 * 144 * c->g.vol;
+  if (ensure(c->staging, bytes)) return -1;
+  if (c->prec == WLG_FP64)
+    soa_to_aos<double>(c->g, view4<double>(c->U.p, c->g.vol), (double*)c->staging.p, 0, 4, c->st);
+  else
+    soa_to_aos<float>(c->g, view4<float>(c->U.p, c->g.vol), (double*)c->staging.p, 0, 4, c->st);
+  WLG_CUDA(cudaMemcpyAsync(aos, c->staging.p, bytes, cudaMemcpyDeviceToHost, c->st));
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  return finish("download_links");
+}
+
+int wlg_upload_openqcd(wlg_ctx* c, const double* ud, const int* ipt) {
+  CTX_BEGIN(c);
+  size_t bytes = (size_t)4 * 144 * c->g.vol;
+  if (ensure(c->staging, bytes) || ensure(c->ipt, sizeof(int) * c->g.vol)) return -1;
+  WLG_CUDA(cudaMemcpyAsync(c->staging.p, ud, bytes, cudaMemcpyHostToDevice, c->st));
+  WLG_CUDA(cudaMemcpyAsync(c->ipt.p, ipt, sizeof(int) * c->g.vol, cudaMemcpyHostToDevice, c->st));
+  if (c->prec == WLG_FP64)
+    openqcd_to_soa<double>(c->g, (const double*)c->staging.p, (const int*)c->ipt.p,
+                           view4<double>(c->U.p, c->g.vol), 0, 4, c->st);
+  else
+    openqcd_to_soa<float>(c->g, (const double*)c->staging.p, (const int*)c->ipt.p,
+                          view4<float>(c->U.p, c->g.vol), 0, 4, c->st);
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  return finish("upload_openqcd");
+}
+
+int wlg_download_openqcd(wlg_ctx* c, double* ud, const int* ipt) {
+  CTX_BEGIN(c);
+  size_t bytes = (size_t)4 * 144 * c->g.vol;
+  if (ensure(c->staging, bytes) || ensure(c->ipt, sizeof(int) * c->g.vol)) return -1;
+  WLG_CUDA(cudaMemcpyAsync(c->ipt.p, ipt, sizeof(int) * c->g.vol, cudaMemcpyHostToDevice, c->st));
+  if (c->prec == WLG_FP64)
+    soa_to_openqcd<double>(c->g, view4<double>(c->U.p, c->g.vol), (const int*)c->ipt.p,
+                           (double*)c->staging.p, 0, 4, c->st);
+  else
+    soa_to_openqcd<float>(c->g, view4<float>(c->U.p, c->g.vol), (const int*)c->ipt.p,
+                          (double*)c->staging.p, 0, 4, c->st);
+  WLG_CUDA(cudaMemcpyAsync(ud, c->staging.p, bytes, cudaMemcpyDeviceToHost, c->st));
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  return finish("download_openqcd");
+}
+
+int wlg_generate(wlg_ctx* c, uint64_t seed, double eps) {
+  CTX_BEGIN(c);
+  if (c->prec == WLG_FP64)
+    generate_soa<double>(c->g, c->bc, seed, eps, view4<double>(c->U.p, c->g.vol), c->st);
+  else
+    generate_soa<float>(c->g, c->bc, seed, eps, view4<float>(c->U.p, c->g.vol), c->st);
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  return finish("generate");
+}
+
+int wlg_hyp(wlg_ctx* c, double a1, double a2, double a3, int proj, int piter, int mu0, int mu1,
+            int keep) {
+  CTX_BEGIN(c);
+  if (mu0 < 0 || mu1 > 4 || mu0 >= mu1) {
+    set_error("hyp: bad direction range [%d,%d)", mu0, mu1);
+    return -1;
+  }
+  int rc = c->prec == WLG_FP64 ? do_hyp<double>(c, a1, a2, a3, proj, piter, mu0, mu1, keep)
+                               : do_hyp<float>(c, a1, a2, a3, proj, piter, mu0, mu1, keep);
+  return rc;
+}
+
+int wlg_ape(wlg_ctx* c, double alpha, int proj, int piter, int time, int nsweeps, int keep) {
+  CTX_BEGIN(c);
+  return c->prec == WLG_FP64 ? do_ape<double>(c, alpha, proj, piter, time, nsweeps, keep)
+                             : do_ape<float>(c, alpha, proj, piter, time, nsweeps, keep);
+}
+
+int wlg_hyp_spatial(wlg_ctx* c, double a1, double a2, int proj, int piter, int nsweeps, int keep) {
+  CTX_BEGIN(c);
+  return c->prec == WLG_FP64 ? do_hyp_spatial<double>(c, a1, a2, proj, piter, nsweeps, keep)
+                             : do_hyp_spatial<float>(c, a1, a2, proj, piter, nsweeps, keep);
+}
+
+int wlg_plaq_sum(wlg_ctx* c, double* out) {
+  CTX_BEGIN(c);
+  if (ensure(c->plaq_out, sizeof(double) * WLG_MAX_SM_LEVELS)) return -1;
+  int rc = c->prec == WLG_FP64
+               ? do_plaq<double>(c, view4<double>(c->U.p, c->g.vol), (double*)c->plaq_out.p)
+               : do_plaq<float>(c, view4<float>(c->U.p, c->g.vol), (double*)c->plaq_out.p);
+  if (rc) return rc;
+  WLG_CUDA(cudaMemcpyAsync(out, c->plaq_out.p, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  return finish("plaq_sum");
+}
+
+int wlg_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, double* plaq) {
+  CTX_BEGIN(c);
+  return c->prec == WLG_FP64 ? do_wloop_sum<double>(c, p, wl_mat, plaq)
+                             : do_wloop_sum<float>(c, p, wl_mat, plaq);
+}
+
+int wlg_measure(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, double* plaq) {
+  CTX_BEGIN(c);
+  if (check_parms(c, p)) return -1;
+  int proj = p->proj_iter > 0;
+  if (wlg_hyp(c, p->alpha_action[0], p->alpha_action[1], p->alpha_action[2], proj, p->proj_iter, 0,
+              4, 1))
+    return -1;
+  return wlg_wloop_sum(c, p, wl_mat, plaq);
+}
+
+int wlg_download_level(wlg_ctx* c, int sl, double* aos3) {
+  CTX_BEGIN(c);
+  if (!c->levels.p || sl < 0 || sl >= c->last_msl) {
+    set_error("level %d not available", sl);
+    return -1;
+  }
+  size_t bytes = (size_t)4 * 144 * c->g.vol;
+  if (ensure(c->staging, bytes)) return -1;
+  // convert to a 4-direction AoS with the temporal slot unused, then compact
+  size_t f3 = field_bytes(c, 3);
+  void* base = (char*)c->levels.p + f3 * sl;
+  if (c->prec == WLG_FP64) {
+    Links<double> L = view3<double>(base, c->g.vol);
+    soa_to_aos<double>(c->g, L, (double*)c->staging.p, 1, 4, c->st);
+  } else {
+    Links<float> L = view3<float>(base, c->g.vol);
+    soa_to_aos<float>(c->g, L, (double*)c->staging.p, 1, 4, c->st);
+  }
+  // AoS [V][4][18] -> [V][3][18]: strided copy of the spatial links
+  WLG_CUDA(cudaMemcpy2DAsync(aos3, 3 * 144, (char*)c->staging.p + 144, 4 * 144, 3 * 144,
+                             c->g.vol, cudaMemcpyDeviceToHost, c->st));
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  return finish("download_level");
+}
+
+int wlg_staple_sum(const int n[4], const double* u1, const double* u2, int mu, int nu, double* vb) {
+  set_error("%s", "");
+  if (mu < 0 || mu > 3 || nu < 0 || nu > 3 || mu == nu) {
+    set_error("staple_sum: need 0<=mu,nu<4 and mu!=nu");
+    return -1;
+  }
+  wlg_ctx* c = nullptr;
+  if (wlg_create(n, 3, WLG_FP64, 0, &c)) return -1;
+  int rc = -1;
+  size_t fb = field_bytes(c, 4);
+  DevBuf b1, b2;
+  do {
+    if (ensure(b1, fb) || ensure(b2, fb)) break;
+    if (wlg_upload_links(c, u1)) break;
+    WLG_CUDA(cudaMemcpyAsync(b1.p, c->U.p, fb, cudaMemcpyDeviceToDevice, c->st));
+    if (wlg_upload_links(c, u2)) break;
+    WLG_CUDA(cudaMemcpyAsync(b2.p, c->U.p, fb, cudaMemcpyDeviceToDevice, c->st));
+    if (wlg_upload_links(c, vb)) break;
+    staple_sum<double>(c->g, view4<double>(b1.p, c->g.vol), view4<double>(b2.p, c->g.vol), mu, nu,
+                       view4<double>(c->U.p, c->g.vol), c->st);
+    if (wlg_download_links(c, vb)) break;
+    rc = 0;
+  } while (0);
+  release(b1);
+  release(b2);
+  wlg_destroy(c);
+  return rc;
+}
+
+int wlg_project(double* mats, int nmat, int iter) {
+  set_error("%s", "");
+  if (nmat <= 0) return 0;
+  if (wlg_device_count() <= 0) {
+    set_error("no CUDA device available (the wloop_b200 path has no CPU fallback)");
+    return -1;
+  }
+  DevBuf b;
+  if (ensure(b, sizeof(double) * 18 * (size_t)nmat)) return -1;
+  WLG_CUDA(cudaMemcpy(b.p, mats, sizeof(double) * 18 * (size_t)nmat, cudaMemcpyHostToDevice));
+  project_batch((double*)b.p, nmat, iter, 0);
+  WLG_CUDA(cudaMemcpy(mats, b.p, sizeof(double) * 18 * (size_t)nmat, cudaMemcpyDeviceToHost));
+  release(b);
+  return finish("project");
+}
+
+int wlg_set_profiling(wlg_ctx* c, int on) {
+  CTX_BEGIN(c);
+  harvest(c);
+  c->prof = on != 0;
+  return 0;
+}
+
+int wlg_kernel_time(wlg_ctx* c, const char* name, double* total_ms, long long* launches) {
+  CTX_BEGIN(c);
+  harvest(c);
+  auto it = c->stats.find(name ? name : "");
+  double ms = 0.0;
+  long long n = 0;
+  if (it != c->stats.end()) {
+    ms = it->second.ms;
+    n = it->second.n;
+  }
+  if (total_ms) *total_ms = ms;
+  if (launches) *launches = n;
+  return 0;
+}
+
+int wlg_reset_kernel_times(wlg_ctx* c) {
+  CTX_BEGIN(c);
+  harvest(c);
+  c->stats.clear();
+  return 0;
+}
+
+int wlg_set_contract_shape(wlg_ctx* c, int G, int nCB, int block) {
+  CTX_BEGIN(c);
+  if (G < 0 || G > 6 || nCB < 0 || (block != 0 && (block % 32 != 0 || block > 1024))) {
+    set_error("bad contraction shape");
+    return -1;
+  }
+  c->cG = G;
+  c->cNCB = nCB;
+  c->cBlock = block;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,125 @@
+// internal.h -- launchers shared between the wloop_b200 translation units.
+// Nothing here is exported; the C-ABI lives in include/wloop_b200.h.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include "common.cuh"
+
+namespace wlg {
+
+// Launch shape for the site-parallel kernels (picked by the autotuner).
+struct Shape {
+  int block;  // threads per block
+  int waves;  // grid = waves * SMs * blocks-per-SM (grid-stride loops)
+};
+
+int num_sms();
+
+// ---- smearing (smear.cu) --------------------------------------------------
+// HYP in three levels (hyp_links.c:194-451).  vbar/vtil hold 3 pair slots x 4
+// directions; U is updated in place for the directions in [mu0,mu1).
+template <class T>
+void hyp_level3(const Geo& g, Links<T> U, typename V2<T>::t* vbar, double a3, int proj, int iter,
+                cudaStream_t st);
+template <class T>
+void hyp_level2(const Geo& g, Links<T> U, const typename V2<T>::t* vbar, typename V2<T>::t* vtil,
+                double a2, int proj, int iter, cudaStream_t st);
+template <class T>
+void hyp_level1(const Geo& g, Links<T> U, const typename V2<T>::t* vtil, double a1, int proj,
+                int iter, int mu0, int mu1, int bc, cudaStream_t st);
+// One APE sweep dst = P[src + alpha * staples] over directions [mu0,4)
+// (ape_links.c:147-272).  dst must not alias src.
+template <class T>
+void ape_sweep(const Geo& g, Links<T> src, Links<T> dst, double alpha, int proj, int iter,
+               int mu0, cudaStream_t st);
+// Two-level spatial HYP (hyp_spatial_links.c:160-344); dl holds 2 slots x 3
+// spatial directions; U's spatial links are updated in place.
+template <class T>
+void hyp3d_level1(const Geo& g, Links<T> U, typename V2<T>::t* dl, double a2, int proj, int iter,
+                  cudaStream_t st);
+template <class T>
+void hyp3d_level2(const Geo& g, Links<T> U, const typename V2<T>::t* dl, double a1, int proj,
+                  int iter, cudaStream_t st);
+// staple_sum (staple_sum.c:53-87): vb(x,mu) += staples in the (mu,nu) plane.
+template <class T>
+void staple_sum(const Geo& g, Links<T> u1, Links<T> u2, int mu, int nu, Links<T> vb,
+                cudaStream_t st);
+// In-place projection of n packed FP64 matrices (18 doubles each).
+void project_batch(double* m, int n, int iter, cudaStream_t st);
+// Plaquette sum (lnkplaq.c:48-128) into *out (device double); partial holds
+// at least plaq_partials() doubles.
+template <class T>
+void plaq_sum(const Geo& g, int bc, Links<T> U, double* partial, double* out, cudaStream_t st);
+int plaq_partials();
+
+// ---- loops (loops.cu) -----------------------------------------------------
+// lines_dst[sl][k] = lines_src[sl][k](x) * level[sl][k](x + (R-1) k)
+template <class T>
+void line_step(const Geo& g, int msl, int R, const typename V2<T>::t* level,
+               const typename V2<T>::t* src, typename V2<T>::t* dst, cudaStream_t st);
+// Contraction for one spatial extent R: partial sums of
+// Re tr(line_s2(x0+T)^dag  U0^dag...  line_s1(x0) ...U0') over columns.
+struct ContractPlan {
+  int G;        // bottom levels per thread
+  int ngrp;     // ceil(msl/G)
+  int nCB;      // column blocks per (x0, group)
+  int block;    // threads per block
+  size_t smem;  // dynamic shared memory bytes
+  size_t partial_doubles;
+};
+ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hint, int nCB_hint,
+                           int block_hint);
+template <class T>
+void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
+              const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
+              cudaStream_t st);
+// Sums the partials and writes wl_mat[wl_idx(s1,s2,t,r,x0)] / norm.
+void contract_reduce(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mwlr, int r,
+                     const double* partial, double* wl_mat, cudaStream_t st);
+
+// ---- layout (layout.cu) ---------------------------------------------------
+// AoS lexicographic FP64 [V][4][18] <-> SoA field of type T (directions [mu0,mu1)).
+template <class T>
+void aos_to_soa(const Geo& g, const double* aos, Links<T> U, int mu0, int mu1, cudaStream_t st);
+template <class T>
+void soa_to_aos(const Geo& g, Links<T> U, double* aos, int mu0, int mu1, cudaStream_t st);
+// openQCD layout (8 links per odd point, lnkcom.c:840-859) <-> SoA; ipt maps
+// lexicographic to openQCD site index.
+template <class T>
+void openqcd_to_soa(const Geo& g, const double* ud, const int* ipt, Links<T> U, int mu0, int mu1,
+                    cudaStream_t st);
+template <class T>
+void soa_to_openqcd(const Geo& g, Links<T> U, const int* ipt, double* ud, int mu0, int mu1,
+                    cudaStream_t st);
+// Copy nlinks*9 complex entries between fields of possibly different precision.
+template <class D, class S>
+void convert(typename V2<D>::t* dst, const typename V2<S>::t* src, size_t n, cudaStream_t st);
+
+// ---- synthetic fields (gen_dev.cu) -----------------------------------------
+// Writes the synthetic link field of the given seed/eps straight into SoA.
+template <class T>
+void generate_soa(const Geo& g, int bc, uint64_t seed, double eps, Links<T> U, cudaStream_t st);
+
+// ---- error handling -------------------------------------------------------
+void set_error(const char* fmt, ...);
+const char* get_error();
+
+}  // namespace wlg
+
+#define WLG_CUDA(call)                                                                    \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) {                                                              \
+      wlg::set_error("%s failed at %s:%d: %s", #call, __FILE__, __LINE__,                 \
+                     cudaGetErrorString(e_));                                             \
+      return -1;                                                                          \
+    }                                                                                     \
+  } while (0)
+
+#define WLG_LAUNCH_CHECK(name)                                                            \
+  do {                                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                                  \
+    if (e_ != cudaSuccess) {                                                              \
+      wlg::set_error("kernel %s: %s", name, cudaGetErrorString(e_));                      \
+    }                                                                                     \
+  } while (0)

@@ -1,0 +1,294 @@
+// loops.cu -- Wilson-loop stage: spatial lines, the fused temporal-line /
+// contraction kernel and its deterministic reduction.
+//
+// The reference (wloop.c:436-508) rebuilds the temporal lines L_T for every
+// T and, for every level pair (sl1,sl2), multiplies two full products per
+// site: msl^2 (2M+36) flops per site and direction.  Here the quantity
+//     W_{s1 s2}(x0,T) = sum_{xs,k} Re tr[ line_s2(x0+T)^dag  C_s1(x0,T) ]
+//     C_s1(x0,T)      = U0(x0+T-1)^dag C_s1(x0,T-1) U0'(x0+T-1),  C_s1(x0,0) = line_s1(x0)
+// (U0 at xs, U0' at xs+R k) is the same trace, Re tr[(ub um)^dag (ul ubR)],
+// with C carried in registers along T: 2 msl M + 36 msl^2 flops.  One thread
+// owns one column (xs,k) at one start slice x0 and G bottom levels; the
+// msl*G traces of each T are summed over the warp by a transposing shuffle
+// reduction and accumulated in a per-warp shared-memory row, so no atomics
+// and a fixed summation order.
+#include "internal.h"
+
+namespace wlg {
+
+// lines_dst[sl][k](x) = lines_src[sl][k](x) * level[sl][k](x + (R-1) k)
+// (compute_uk_long, wloop.c:207-258, multiplied from the other end so the
+// update is in place).
+template <class T>
+__global__ void __launch_bounds__(128) k_line_step(Geo g, int msl, int R,
+                                                   const typename V2<T>::t* level,
+                                                   const typename V2<T>::t* src,
+                                                   typename V2<T>::t* dst) {
+  const long long n = (long long)msl * 3 * g.vol;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
+       w += (long long)gridDim.x * blockDim.x) {
+    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+    int k = q % 3;
+    int x[4];
+    coords(g, s, x);
+    int y = shift(g, s, x[k + 1], k + 1, (R - 1) % g.n[k + 1]);
+    M3<T> a, b, c;
+    ld(a, src + (size_t)q * 9 * g.vol, g.vol, s);
+    ld(b, level + (size_t)q * 9 * g.vol, g.vol, y);
+    mul(c, a, b);
+    st(dst + (size_t)q * 9 * g.vol, g.vol, s, c);
+  }
+}
+
+template <class T>
+void line_step(const Geo& g, int msl, int R, const typename V2<T>::t* level,
+               const typename V2<T>::t* src, typename V2<T>::t* dst, cudaStream_t st) {
+  long long n = (long long)msl * 3 * g.vol;
+  long long grid = (n + 127) / 128;
+  if (grid > num_sms() * 32) grid = num_sms() * 32;
+  k_line_step<T><<<(int)grid, 128, 0, st>>>(g, msl, R, level, src, dst);
+  WLG_LAUNCH_CHECK("line_step");
+}
+
+// ---------------------------------------------------------------------------
+// warp transposing reduction: every lane holds KP values; afterwards lane l
+// holds the warp sum of value index (l >> (5 - log2 KP)).
+// ---------------------------------------------------------------------------
+template <int KP> struct Log2;
+template <> struct Log2<1> { enum { v = 0 }; };
+template <> struct Log2<2> { enum { v = 1 }; };
+template <> struct Log2<4> { enum { v = 2 }; };
+template <> struct Log2<8> { enum { v = 3 }; };
+template <> struct Log2<16> { enum { v = 4 }; };
+template <> struct Log2<32> { enum { v = 5 }; };
+
+template <int KP>
+__device__ __forceinline__ double wt_reduce(double (&v)[KP], int lane) {
+  constexpr int L = Log2<KP>::v;
+#pragma unroll
+  for (int st = 0; st < 5; st++) {
+    const int off = 16 >> st;
+    if (st < L) {
+      const int h = KP >> (st + 1);
+      const bool upper = (lane & off) != 0;
+#pragma unroll
+      for (int i = 0; i < h; i++) {
+        double send = upper ? v[i] : v[i + h];
+        double keep = upper ? v[i + h] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+      }
+    } else {
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], off);
+    }
+  }
+  return v[0];
+}
+
+template <int K> struct Pow2 { enum { v = (K <= 1) ? 1 : (K <= 2) ? 2 : (K <= 4) ? 4 : (K <= 8) ? 8 : (K <= 16) ? 16 : 32 }; };
+
+// ---------------------------------------------------------------------------
+// contraction kernel
+//   grid.x = N0 * ngrp * nCB   (x0 fastest: concurrent blocks share columns)
+//   partial[((x0*ngrp + grp)*nCB + cb)][T][g][s2]
+// ---------------------------------------------------------------------------
+template <class T, int G, int SB>
+__global__ void __launch_bounds__(128) k_contract(Geo g, const typename V2<T>::t* __restrict__ u0,
+                                                  const typename V2<T>::t* __restrict__ lines,
+                                                  int msl, int mwlt, int R, int ngrp, int nCB,
+                                                  double* __restrict__ partial) {
+  extern __shared__ double acc[];  // [nwarps][mwlt][G][msl]
+  constexpr int K = G * SB;
+  constexpr int KP = Pow2<K>::v;
+  static_assert(K <= 32, "G*SB must not exceed 32");
+
+  const int N0 = g.n[0], vs = g.vs, vol = g.vol;
+  int b = blockIdx.x;
+  const int x0 = b % N0;
+  b /= N0;
+  const int grp = b % ngrp;
+  const int cb = b / ngrp;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int rowlen = mwlt * G * msl;
+  double* wacc = acc + (size_t)warp * rowlen;
+  for (int i = lane; i < rowlen; i += 32) wacc[i] = 0.0;
+  __syncwarp();
+
+  const int s1_0 = grp * G;
+  const int ncol = 3 * vs;
+  const int per = (ncol + nCB - 1) / nCB;
+  const int c_begin = cb * per;
+  const int c_end = min(ncol, c_begin + per);
+  const size_t fstride = (size_t)9 * vol;
+
+  // all lanes of a warp iterate together so shuffles stay converged
+  for (int cbase = c_begin; cbase < c_end; cbase += blockDim.x) {
+    const int col = cbase + threadIdx.x;
+    const bool active = col < c_end;
+    const int cc = active ? col : c_begin;
+    const int k = cc / vs, xs = cc - k * vs;
+    // xs + R k (coordinates inside the time slice)
+    int x1 = xs / g.st[1], r = xs - x1 * g.st[1];
+    int x2 = r / g.st[2], x3 = r - x2 * g.st[2];
+    int xsR;
+    {
+      int xx[3] = {x1, x2, x3};
+      int y = xx[k] + (R % g.n[k + 1]);
+      if (y >= g.n[k + 1]) y -= g.n[k + 1];
+      xx[k] = y;
+      xsR = xx[0] * g.st[1] + xx[1] * g.st[2] + xx[2];
+    }
+    M3<T> C[G];
+#pragma unroll
+    for (int gi = 0; gi < G; gi++) {
+      int s1 = min(s1_0 + gi, msl - 1);
+      ld(C[gi], lines + ((size_t)s1 * 3 + k) * fstride, vol, x0 * vs + xs);
+    }
+    int t0 = x0;
+    for (int tt = 1; tt <= mwlt; tt++) {
+      M3<T> u, tmp;
+      ld(u, u0, vol, t0 * vs + xs);
+#pragma unroll
+      for (int gi = 0; gi < G; gi++) {
+        mul_da(tmp, u, C[gi]);
+        C[gi] = tmp;
+      }
+      ld(u, u0, vol, t0 * vs + xsR);
+#pragma unroll
+      for (int gi = 0; gi < G; gi++) {
+        mul(tmp, C[gi], u);
+        C[gi] = tmp;
+      }
+      t0 = (t0 + 1 == N0) ? 0 : t0 + 1;  // = x0+T mod N0, the top slice
+      const int stop = t0 * vs + xs;
+      for (int sb = 0; sb < msl; sb += SB) {
+        double v[KP];
+#pragma unroll
+        for (int i = 0; i < KP; i++) v[i] = 0.0;
+#pragma unroll
+        for (int j = 0; j < SB; j++) {
+          const int s2 = sb + j;
+          if (s2 < msl) {
+            M3<T> l;
+            ld(l, lines + ((size_t)s2 * 3 + k) * fstride, vol, stop);
+#pragma unroll
+            for (int gi = 0; gi < G; gi++) v[gi * SB + j] = active ? (double)retr_dag(l, C[gi]) : 0.0;
+          }
+        }
+        double sum = wt_reduce<KP>(v, lane);
+        const int idx = lane >> (5 - Log2<KP>::v);
+        if ((lane & ((32 / KP) - 1)) == 0 && idx < K) {
+          const int gi = idx / SB, s2 = sb + idx % SB;
+          if (s2 < msl) wacc[((tt - 1) * G + gi) * msl + s2] += sum;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  double* out = partial + (size_t)blockIdx.x * rowlen;
+  for (int i = threadIdx.x; i < rowlen; i += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < nwarps; w++) s += acc[(size_t)w * rowlen + i];
+    out[i] = s;
+  }
+}
+
+ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hint, int nCB_hint,
+                           int block_hint) {
+  ContractPlan p;
+  int G = G_hint;
+  if (G <= 0) {
+    if (fp64) {
+      G = (msl % 3 == 0 || msl > 4) ? 3 : (msl >= 2 ? 2 : 1);
+      if (msl == 4) G = 2;
+    } else {
+      G = msl <= 6 ? msl : (msl % 4 == 0 ? 4 : 4);
+    }
+  }
+  if (G > msl) G = msl;
+  if (G < 1) G = 1;
+  p.G = G;
+  p.ngrp = (msl + G - 1) / G;
+  p.block = block_hint > 0 ? block_hint : 128;
+  int ncol = 3 * g.vs;
+  int nCB = nCB_hint;
+  if (nCB <= 0) {
+    long long want = (long long)num_sms() * 8;
+    long long base = (long long)g.n[0] * p.ngrp;
+    nCB = (int)((want + base - 1) / base);
+    int maxcb = (ncol + p.block - 1) / p.block;
+    if (nCB > maxcb) nCB = maxcb;
+    if (nCB < 1) nCB = 1;
+  }
+  p.nCB = nCB;
+  p.smem = (size_t)(p.block / 32) * mwlt * G * msl * sizeof(double);
+  p.partial_doubles = (size_t)g.n[0] * p.ngrp * nCB * mwlt * G * msl;
+  return p;
+}
+
+template <class T, int G>
+static void launch_contract_G(const Geo& g, const ContractPlan& p,
+                              const typename V2<T>::t* u0, const typename V2<T>::t* lines,
+                              int msl, int mwlt, int R, double* partial, cudaStream_t st) {
+  constexpr int SB = (32 / G) < 8 ? (32 / G) : 8;
+  auto kern = k_contract<T, G, SB>;
+  if (p.smem > 48 * 1024)
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+  int grid = g.n[0] * p.ngrp * p.nCB;
+  kern<<<grid, p.block, p.smem, st>>>(g, u0, lines, msl, mwlt, R, p.ngrp, p.nCB, partial);
+  WLG_LAUNCH_CHECK("contract");
+}
+
+template <class T>
+void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
+              const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
+              cudaStream_t st) {
+  switch (p.G) {
+    case 1: launch_contract_G<T, 1>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 2: launch_contract_G<T, 2>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 3: launch_contract_G<T, 3>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 4: launch_contract_G<T, 4>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 5: launch_contract_G<T, 5>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 6: launch_contract_G<T, 6>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    default: set_error("contract: unsupported G=%d", p.G);
+  }
+}
+
+// wl_mat[sl1 + msl*(sl2 + msl*(t + mwlt*(r + mwlr*x0)))] (wloop_parms.c:431-434)
+__global__ void k_contract_reduce(int N0, int msl, int mwlt, int mwlr, int r, int G, int ngrp,
+                                  int nCB, double norm, const double* __restrict__ partial,
+                                  double* __restrict__ wl) {
+  const int nout = N0 * mwlt * msl * msl;
+  const int rowlen = mwlt * G * msl;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nout; i += gridDim.x * blockDim.x) {
+    int s1 = i % msl, q = i / msl;
+    int s2 = q % msl;
+    q /= msl;
+    int t = q % mwlt, x0 = q / mwlt;
+    int grp = s1 / G, gi = s1 - grp * G;
+    const double* p = partial + (size_t)((x0 * ngrp + grp) * nCB) * rowlen + (t * G + gi) * msl + s2;
+    double s = 0.0;
+    for (int cb = 0; cb < nCB; cb++) s += p[(size_t)cb * rowlen];
+    wl[s1 + msl * (s2 + msl * (t + mwlt * (r + mwlr * x0)))] = s / norm;
+  }
+}
+
+void contract_reduce(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mwlr, int r,
+                     const double* partial, double* wl_mat, cudaStream_t st) {
+  int nout = g.n[0] * mwlt * msl * msl;
+  int grid = (nout + 255) / 256;
+  double norm = 9.0 * (double)g.n[1] * (double)g.n[2] * (double)g.n[3];  // wloop.c:535
+  k_contract_reduce<<<grid, 256, 0, st>>>(g.n[0], msl, mwlt, mwlr, r, p.G, p.ngrp, p.nCB,
+                                          norm, partial, wl_mat);
+  WLG_LAUNCH_CHECK("contract_reduce");
+}
+
+template void line_step<double>(const Geo&, int, int, const double2*, const double2*, double2*,
+                                cudaStream_t);
+template void line_step<float>(const Geo&, int, int, const float2*, const float2*, float2*,
+                               cudaStream_t);
+template void contract<double>(const Geo&, const ContractPlan&, const double2*, const double2*, int,
+                               int, int, double*, cudaStream_t);
+template void contract<float>(const Geo&, const ContractPlan&, const float2*, const float2*, int,
+                              int, int, double*, cudaStream_t);
+
+}  // namespace wlg

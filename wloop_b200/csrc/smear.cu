@@ -1,0 +1,413 @@
+// smear.cu -- link smearing kernels for sm_100a.
+//
+// All kernels are one-thread-per-output-link, grid-stride over
+// (output slot, site) with the site fastest, so every component load of a
+// warp is a coalesced SoA request.  Neighbour links are read through the
+// read-only path (__ldg): the staple of link (x,mu) touches links within one
+// lattice row of x, so the L2 (126 MB) serves the re-reads and HBM sees each
+// input field roughly once per kernel.  Staple products run in T (FP64, or
+// FP32 in the mixed form); the linear combination and the SU(3) projection
+// always run in FP64.
+#include "internal.h"
+
+namespace wlg {
+
+// unordered pair index used by hyp_links.c:128-139:
+// {0,1},{2,3} -> 0; {0,2},{1,3} -> 1; {0,3},{1,2} -> 2
+__device__ __forceinline__ int hyp_pair(int a, int b) {
+  int d = a + b;
+  if (d > 3) d = 6 - d;
+  return d - 1;
+}
+
+// dlnks_idx of hyp_spatial_links.c:117-125 (not symmetric)
+__device__ __forceinline__ int hyp3_slot(int mu, int eta) {
+  // [1][2]=0 [1][3]=1 [2][1]=0 [2][3]=1 [3][1]=0 [3][2]=1
+  if (mu == 3) return (eta == 1) ? 0 : 1;
+  return (eta == 3) ? 1 : 0;
+}
+
+static inline int grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  long long cap = (long long)num_sms() * 32;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+template <class T>
+__device__ __forceinline__ typename V2<T>::t* fld(typename V2<T>::t* base, int vol, int slot, int mu,
+                                                  int ndir) {
+  return base + (size_t)(slot * ndir + mu) * 9 * vol;
+}
+
+// v = a*u + b*s (FP64), then optional projection; this is _su3_lcomb +
+// approx_project_to_su3_dble of decorate_all (hyp_links.c:154-171).
+template <class T>
+__device__ __forceinline__ void lcomb_project(M3<double>& v, double a, const M3<T>& u, double b,
+                                              const M3<T>& s, int proj, int iter) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    v.e[k].x = a * (double)u.e[k].x + b * (double)s.e[k].x;
+    v.e[k].y = a * (double)u.e[k].y + b * (double)s.e[k].y;
+  }
+  if (proj) project(v, iter);
+}
+
+// ---------------------------------------------------------------------------
+// HYP level with alpha3 (decorated_links1, hyp_links.c:320-373):
+//   vbar[p(mu,eta)](x,mu) = P[(1-a3) U + a3/2 * S_eta(U)]
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(128) k_hyp_l3(Geo g, Links<T> U, typename V2<T>::t* vbar,
+                                                double a, double b, int proj, int iter) {
+  const long long n = 12LL * g.vol;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
+       w += (long long)gridDim.x * blockDim.x) {
+    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+    int mu = q / 3, eta = (mu + 1 + q % 3) & 3;
+    int x[4];
+    coords(g, s, x);
+    M3<T> S, u;
+    zero(S);
+    add_staples(S, g, x, s, U.p[eta], U.p[mu], mu, eta);
+    ld(u, U.p[mu], g.vol, s);
+    M3<double> v;
+    lcomb_project(v, a, u, b, S, proj, iter);
+    M3<T> o;
+    cvt(o, v);
+    st(fld<T>(vbar, g.vol, hyp_pair(mu, eta), mu, 4), g.vol, s, o);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// HYP level with alpha2 (decorated_links2, hyp_links.c:244-317):
+//   vtil[p(mu,nu)](x,mu) = P[(1-a2) U + a2/4 * sum_{rho != mu,nu} S_rho]
+//   rho-links from vbar[p(mu,nu)], mu-links from vbar[p(nu,rho)]
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(128) k_hyp_l2(Geo g, Links<T> U, const typename V2<T>::t* vbar,
+                                                typename V2<T>::t* vtil, double a, double b,
+                                                int proj, int iter) {
+  const long long n = 12LL * g.vol;
+  typename V2<T>::t* vb = const_cast<typename V2<T>::t*>(vbar);
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
+       w += (long long)gridDim.x * blockDim.x) {
+    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+    int mu = q / 3, nu = (mu + 1 + q % 3) & 3;
+    int x[4];
+    coords(g, s, x);
+    int pmn = hyp_pair(mu, nu);
+    M3<T> S, u;
+    zero(S);
+#pragma unroll
+    for (int rho = 0; rho < 4; rho++) {
+      if (rho == mu || rho == nu) continue;
+      add_staples(S, g, x, s, fld<T>(vb, g.vol, pmn, rho, 4),
+                  fld<T>(vb, g.vol, hyp_pair(nu, rho), mu, 4), mu, rho);
+    }
+    ld(u, U.p[mu], g.vol, s);
+    M3<double> v;
+    lcomb_project(v, a, u, b, S, proj, iter);
+    M3<T> o;
+    cvt(o, v);
+    st(fld<T>(vtil, g.vol, pmn, mu, 4), g.vol, s, o);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// HYP level with alpha1 (decorated_links3, hyp_links.c:194-241) and the copy
+// back into the gauge field (:432-447).  U is written in place: each thread
+// reads only its own U(x,mu) for the linear combination.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(128) k_hyp_l1(Geo g, Links<T> U, const typename V2<T>::t* vtil,
+                                                double a, double b, int proj, int iter, int mu0,
+                                                int nmu, int bc) {
+  const long long n = (long long)nmu * g.vol;
+  typename V2<T>::t* vt = const_cast<typename V2<T>::t*>(vtil);
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
+       w += (long long)gridDim.x * blockDim.x) {
+    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+    int mu = mu0 + q;
+    int x[4];
+    coords(g, s, x);
+    M3<T> S, u;
+    zero(S);
+#pragma unroll
+    for (int i = 1; i < 4; i++) {
+      int nu = (mu + i) & 3, p = hyp_pair(mu, nu);
+      add_staples(S, g, x, s, fld<T>(vt, g.vol, p, nu, 4), fld<T>(vt, g.vol, p, mu, 4), mu, nu);
+    }
+    ld(u, U.p[mu], g.vol, s);
+    M3<double> v;
+    lcomb_project(v, a, u, b, S, proj, iter);
+    M3<T> o;
+    cvt(o, v);
+    if (bc == 0 && mu == 0 && x[0] == g.n[0] - 1) zero(o);  // set_bc(), open bc
+    st(U.p[mu], g.vol, s, o);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One APE sweep (ape_links_all, ape_links.c:217-272):
+//   dst(x,mu) = P[src(x,mu) + alpha * sum_{eta != mu} S_eta(src)]
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(128) k_ape(Geo g, Links<T> src, Links<T> dst, double alpha,
+                                             int proj, int iter, int mu0) {
+  const int nd = 4 - mu0;
+  const long long n = (long long)nd * g.vol;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
+       w += (long long)gridDim.x * blockDim.x) {
+    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+    int mu = mu0 + q;
+    int x[4];
+    coords(g, s, x);
+    M3<T> S, u;
+    zero(S);
+    for (int eta = mu0; eta < 4; eta++) {
+      if (eta == mu) continue;
+      add_staples(S, g, x, s, src.p[eta], src.p[mu], mu, eta);
+    }
+    ld(u, src.p[mu], g.vol, s);
+    M3<double> v;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {  // _su3_mulr then _su3_add (:246-247)
+      double sr = alpha * (double)S.e[k].x, si = alpha * (double)S.e[k].y;
+      v.e[k].x = (double)u.e[k].x + sr;
+      v.e[k].y = (double)u.e[k].y + si;
+    }
+    if (proj) project(v, iter);
+    M3<T> o;
+    cvt(o, v);
+    st(dst.p[mu], g.vol, s, o);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Spatial HYP, level with alpha2 (decorated_links1, hyp_spatial_links.c:210-265)
+//   dl[slot(mu,eta)](x,mu) = P[(1-a2) U + a2/2 S_eta(U)]
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(128) k_hyp3_l1(Geo g, Links<T> U, typename V2<T>::t* dl,
+                                                 double a, double b, int proj, int iter) {
+  const long long n = 6LL * g.vol;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
+       w += (long long)gridDim.x * blockDim.x) {
+    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+    int mu = 1 + q / 2, eta = ((mu + q % 2) % 3) + 1;
+    int x[4];
+    coords(g, s, x);
+    M3<T> S, u;
+    zero(S);
+    add_staples(S, g, x, s, U.p[eta], U.p[mu], mu, eta);
+    ld(u, U.p[mu], g.vol, s);
+    M3<double> v;
+    lcomb_project(v, a, u, b, S, proj, iter);
+    M3<T> o;
+    cvt(o, v);
+    st(fld<T>(dl, g.vol, hyp3_slot(mu, eta), mu - 1, 3), g.vol, s, o);
+  }
+}
+
+// Spatial HYP, level with alpha1 (decorated_links2, hyp_spatial_links.c:160-207)
+template <class T>
+__global__ void __launch_bounds__(128) k_hyp3_l2(Geo g, Links<T> U, const typename V2<T>::t* dl_,
+                                                 double a, double b, int proj, int iter) {
+  const long long n = 3LL * g.vol;
+  typename V2<T>::t* dl = const_cast<typename V2<T>::t*>(dl_);
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
+       w += (long long)gridDim.x * blockDim.x) {
+    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+    int mu = 1 + q;
+    int x[4];
+    coords(g, s, x);
+    M3<T> S, u;
+    zero(S);
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      int nu = ((mu + i) % 3) + 1;
+      add_staples(S, g, x, s, fld<T>(dl, g.vol, hyp3_slot(nu, mu), nu - 1, 3),
+                  fld<T>(dl, g.vol, hyp3_slot(mu, nu), mu - 1, 3), mu, nu);
+    }
+    ld(u, U.p[mu], g.vol, s);
+    M3<double> v;
+    lcomb_project(v, a, u, b, S, proj, iter);
+    M3<T> o;
+    cvt(o, v);
+    st(U.p[mu], g.vol, s, o);
+  }
+}
+
+// staple_sum: vb(x,mu) += up + down staples in the (mu,nu) plane
+template <class T>
+__global__ void k_staple_sum(Geo g, Links<T> u1, Links<T> u2, int mu, int nu, Links<T> vb) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < g.vol; s += gridDim.x * blockDim.x) {
+    int x[4];
+    coords(g, s, x);
+    M3<T> v;
+    ld(v, vb.p[mu], g.vol, s);
+    add_staples(v, g, x, s, u1.p[nu], u2.p[mu], mu, nu);
+    st(vb.p[mu], g.vol, s, v);
+  }
+}
+
+__global__ void k_project_batch(double* m, int n, int iter) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    M3<double> u;
+    const double2* p = reinterpret_cast<const double2*>(m + 18 * (size_t)i);
+#pragma unroll
+    for (int c = 0; c < 9; c++) u.e[c] = p[c];
+    project(u, iter);
+    double2* q = reinterpret_cast<double2*>(m + 18 * (size_t)i);
+#pragma unroll
+    for (int c = 0; c < 9; c++) q[c] = u.e[c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plaquette sum (local_plaq_sum_dble, lnkplaq.c:68-114): per site the (mu,0)
+// plaquettes (skipped at x0=N0-1 for open bc) and the (mu,nu) spatial ones,
+// products in T, sums in FP64; warp shuffle + block reduction into one
+// partial per block, then a fixed-order final pass (deterministic).
+// ---------------------------------------------------------------------------
+constexpr int kPlaqBlocks = 1184;  // 8 x 148 SMs
+constexpr int kPlaqThreads = 256;
+int plaq_partials() { return kPlaqBlocks; }
+
+template <class T>
+__device__ __forceinline__ double plaq_at(const Geo& g, const Links<T>& U, const int x[4], int s,
+                                          int mu, int nu) {
+  M3<T> a, b, w1, w2;
+  ld(a, U.p[mu], g.vol, s);
+  ld(b, U.p[nu], g.vol, up(g, s, x[mu], mu));
+  mul(w1, a, b);
+  ld(a, U.p[nu], g.vol, s);
+  ld(b, U.p[mu], g.vol, up(g, s, x[nu], nu));
+  mul(w2, a, b);
+  return (double)retr_dag(w1, w2);
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (wid == 0) {
+    r = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+  }
+  __syncthreads();
+  return r;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kPlaqThreads) k_plaq(Geo g, int bc, Links<T> U, double* partial) {
+  double acc = 0.0;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < g.vol; s += gridDim.x * blockDim.x) {
+    int x[4];
+    coords(g, s, x);
+    double pa = 0.0;
+    for (int mu = 1; mu < 4; mu++) {
+      if (x[0] < g.n[0] - 1 || bc != 0) pa += plaq_at(g, U, x, s, mu, 0);
+      for (int nu = 1; nu < mu; nu++) pa += plaq_at(g, U, x, s, mu, nu);
+    }
+    acc += pa;
+  }
+  double r = block_sum(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = r;
+}
+
+__global__ void k_sum_partials(const double* partial, int n, double* out) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+  double r = block_sum(acc);
+  if (threadIdx.x == 0) *out = r;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <class T>
+void hyp_level3(const Geo& g, Links<T> U, typename V2<T>::t* vbar, double a3, int proj, int iter,
+                cudaStream_t st) {
+  k_hyp_l3<T><<<grid_for(12LL * g.vol, 128), 128, 0, st>>>(g, U, vbar, 1.0 - a3, a3 / 2.0, proj,
+                                                           iter);
+  WLG_LAUNCH_CHECK("hyp_level3");
+}
+template <class T>
+void hyp_level2(const Geo& g, Links<T> U, const typename V2<T>::t* vbar, typename V2<T>::t* vtil,
+                double a2, int proj, int iter, cudaStream_t st) {
+  k_hyp_l2<T><<<grid_for(12LL * g.vol, 128), 128, 0, st>>>(g, U, vbar, vtil, 1.0 - a2, a2 / 4.0,
+                                                           proj, iter);
+  WLG_LAUNCH_CHECK("hyp_level2");
+}
+template <class T>
+void hyp_level1(const Geo& g, Links<T> U, const typename V2<T>::t* vtil, double a1, int proj,
+                int iter, int mu0, int mu1, int bc, cudaStream_t st) {
+  int nmu = mu1 - mu0;
+  if (nmu <= 0) return;
+  k_hyp_l1<T><<<grid_for((long long)nmu * g.vol, 128), 128, 0, st>>>(g, U, vtil, 1.0 - a1, a1 / 6.0,
+                                                                     proj, iter, mu0, nmu, bc);
+  WLG_LAUNCH_CHECK("hyp_level1");
+}
+template <class T>
+void ape_sweep(const Geo& g, Links<T> src, Links<T> dst, double alpha, int proj, int iter, int mu0,
+               cudaStream_t st) {
+  k_ape<T><<<grid_for((long long)(4 - mu0) * g.vol, 128), 128, 0, st>>>(g, src, dst, alpha, proj,
+                                                                          iter, mu0);
+  WLG_LAUNCH_CHECK("ape_sweep");
+}
+template <class T>
+void hyp3d_level1(const Geo& g, Links<T> U, typename V2<T>::t* dl, double a2, int proj, int iter,
+                  cudaStream_t st) {
+  k_hyp3_l1<T><<<grid_for(6LL * g.vol, 128), 128, 0, st>>>(g, U, dl, 1.0 - a2, a2 / 2.0, proj, iter);
+  WLG_LAUNCH_CHECK("hyp3d_level1");
+}
+template <class T>
+void hyp3d_level2(const Geo& g, Links<T> U, const typename V2<T>::t* dl, double a1, int proj,
+                  int iter, cudaStream_t st) {
+  k_hyp3_l2<T><<<grid_for(3LL * g.vol, 128), 128, 0, st>>>(g, U, dl, 1.0 - a1, a1 / 4.0, proj, iter);
+  WLG_LAUNCH_CHECK("hyp3d_level2");
+}
+template <class T>
+void staple_sum(const Geo& g, Links<T> u1, Links<T> u2, int mu, int nu, Links<T> vb,
+                cudaStream_t st) {
+  k_staple_sum<T><<<grid_for(g.vol, 128), 128, 0, st>>>(g, u1, u2, mu, nu, vb);
+  WLG_LAUNCH_CHECK("staple_sum");
+}
+void project_batch(double* m, int n, int iter, cudaStream_t st) {
+  if (n <= 0) return;
+  k_project_batch<<<grid_for(n, 128), 128, 0, st>>>(m, n, iter);
+  WLG_LAUNCH_CHECK("project_batch");
+}
+template <class T>
+void plaq_sum(const Geo& g, int bc, Links<T> U, double* partial, double* out, cudaStream_t st) {
+  k_plaq<T><<<kPlaqBlocks, kPlaqThreads, 0, st>>>(g, bc, U, partial);
+  WLG_LAUNCH_CHECK("plaq_sum");
+  k_sum_partials<<<1, 1024, 0, st>>>(partial, kPlaqBlocks, out);
+  WLG_LAUNCH_CHECK("plaq_sum_final");
+}
+
+#define WLG_INST(T)                                                                               \
+  template void hyp_level3<T>(const Geo&, Links<T>, V2<T>::t*, double, int, int, cudaStream_t);   \
+  template void hyp_level2<T>(const Geo&, Links<T>, const V2<T>::t*, V2<T>::t*, double, int, int, \
+                              cudaStream_t);                                                      \
+  template void hyp_level1<T>(const Geo&, Links<T>, const V2<T>::t*, double, int, int, int, int,  \
+                              int, cudaStream_t);                                                 \
+  template void ape_sweep<T>(const Geo&, Links<T>, Links<T>, double, int, int, int, cudaStream_t); \
+  template void hyp3d_level1<T>(const Geo&, Links<T>, V2<T>::t*, double, int, int, cudaStream_t); \
+  template void hyp3d_level2<T>(const Geo&, Links<T>, const V2<T>::t*, double, int, int,          \
+                                cudaStream_t);                                                    \
+  template void staple_sum<T>(const Geo&, Links<T>, Links<T>, int, int, Links<T>, cudaStream_t);  \
+  template void plaq_sum<T>(const Geo&, int, Links<T>, double*, double*, cudaStream_t);
+
+WLG_INST(double)
+WLG_INST(float)
+
+}  // namespace wlg
