@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Headline benchmark: Wilson-loop measurements (configs/s) at 32^3x64.
+
+One step = one full measurement of one synthetic 32^3x64 configuration, the
+work ms10's set_data does per configuration (main/ms10.c:633-646):
+HYP2 smearing of all links, 6 APE levels (nss 0 10 10 10 10 10, alpha 0.5),
+and the 6x6 Wilson-loop matrices for r <= 16, t <= 24 on every time slice.
+The headline form is mixed precision (FP32 links / staples / line products,
+FP64 projection and sums); the FP64 form runs the same workload and the
+per-entry error of the mixed result against it is reported.
+
+  value    configs/s with the input field resident in HBM (device-to-device
+           restore of the unsmeared field at the start of each step)
+  e2e      configs/s through the public API from a pinned host buffer: the
+           FP64 su3_dble field (H2D) in, the wl_mat (D2H) out, every step
+  roofline the Wilson-loop contraction kernel (the dominant kernel), its
+           algorithmic flops per launch over its CUDA-event time
+
+Multi-GPU (torchrun): independent replicas, one configuration stream per
+GPU, no collective on the data path ("scaling": "weak").
+
+--impl reference times the reference algorithm's CPU implementation (the
+FP64 oracle port, since the reference itself cannot be built here) on a
+bounded sample of the same workload on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "configs/s at 32^3x64, mixed vs FP64 GPU at <=1e-6 rel err; p50/p99 latency"
+UNIT = "configs/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--skip-fp64", action="store_true", help="do not run the FP64 comparison")
+    ap.add_argument("--skip-cpu", action="store_true", help="do not time the CPU baseline")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--lattice", default=None,
+                    help="N0xN1xN2xN3 override for small profiling captures (not a bench line)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU side: bounded, stage-wise sample of the reference algorithm (oracle)
+# ---------------------------------------------------------------------------
+def cpu_sample(ns: int, nt: int, threads: int):
+    """Times the FP64 oracle (the reference algorithm restated) on an
+    ns^3 x nt lattice with the workload's per-site parameters: HYP once, one
+    APE sweep, and the loop stage for r,t <= 4 with msl 6.  Every stage is
+    linear in the volume, APE in the sweep count, and the reference's
+    loop contraction costs the same per (r,t) pair (wloop.c:545-571), so
+    t_config = (V/V_s) (t_hyp + 50 t_ape + (16*24/16) t_loop)."""
+    from tests import oracle as O  # checker / baseline only
+    from wloop_b200.api import WloopParms, generate_links
+    from wloop_b200.workloads import C3
+    O.set_threads(threads)
+    n = (nt, ns, ns, ns)
+    u = generate_links(n, 3, 3, 0.2)
+    t0 = time.perf_counter()
+    uh = O.hyp_links(n, 3, u, 1.0, 1.0, 0.5, 1, 4)
+    t1 = time.perf_counter()
+    O.ape_links(n, uh, 0.5, 1, 4, time=0, nsweeps=1)
+    t2 = time.perf_counter()
+    p = WloopParms(msl=6, nss=[0] * 6, mwlt=4, mwlr=4, alpha_ape=0.5, proj_iter=4)
+    O.wloop_sum(n, 3, uh, p)
+    t3 = time.perf_counter()
+    c3 = C3.parms
+    scale_v = C3.volume / float(nt * ns ** 3)
+    sweeps = sum(c3.nss[:c3.msl])
+    pairs = (c3.mwlr * c3.mwlt) / 16.0
+    t_cfg = scale_v * ((t1 - t0) + sweeps * (t2 - t1) + pairs * (t3 - t2))
+    sample = (f"oracle on {ns}^3x{nt} (1/{scale_v:.1f} of the volume): HYP once "
+              f"{t1 - t0:.2f}s, one APE sweep {t2 - t1:.2f}s, loops r,t<=4 msl 6 {t3 - t2:.2f}s; "
+              f"scaled by volume, {sweeps} sweeps and {pairs:.0f}x the (r,t) pairs")
+    return 1.0 / t_cfg, t3 - t0, sample
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    times, samples = [], ""
+    for i in range(args.warmup + args.steps):
+        v, wall, samples = cpu_sample(12, 24, threads)
+        if i >= args.warmup:
+            times.append(1.0 / v)
+    t = statistics.mean(times)
+    value = 1.0 / t
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "c3: 32^3x64 periodic, HYP2, APE 0.5 nss 0 10 10 10 10 10, "
+                                   "msl 6, r<=16, t<=24", "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": samples},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "contract_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+    from wloop_b200.api import Context, launch_count, peak_tflops
+    from wloop_b200.workloads import C3, flops_per_config
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier_max(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    w = C3
+    if args.lattice:
+        import dataclasses
+        n = tuple(int(x) for x in args.lattice.split("x"))
+        pp = dataclasses.replace(w.parms, mwlt=min(w.parms.mwlt, n[0] // 2 + 1),
+                                 mwlr=min(w.parms.mwlr, n[1] // 2 + 1))
+        w = dataclasses.replace(w, n=n, parms=pp)
+    p = w.parms
+    fl = flops_per_config(w)
+
+    def timed_value(prec, steps, warmup, profile):
+        ctx = Context(w.n, w.bc, prec, device=local)
+        ctx.generate(w.seed + 1000 * rank, w.eps)
+        ctx.snapshot()
+        for _ in range(warmup):
+            ctx.restore()
+            ctx.measure(p)
+        ext = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx.reset_kernel_times()
+        ctx.set_profiling(profile)
+        clocks = ClockSampler(local)
+        barrier()
+        torch.cuda.synchronize(local)
+        clocks.start()
+        l0 = launch_count()
+        e0.record(ext)
+        wl = None
+        for _ in range(steps):
+            ctx.restore()
+            wl = ctx.measure(p)
+        e1.record(ext)
+        e1.synchronize()
+        torch.cuda.synchronize(local)
+        l1 = launch_count()
+        ck = clocks.stop()
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        kt = {k: ctx.kernel_time(k) for k in ("hyp", "ape", "plaq", "lines", "contract", "reduce")}
+        ctx.set_profiling(False)
+        return ctx, ms, wl, kt, ck, l1 - l0
+
+    # ---- headline precision: device-resident value ----
+    ctx, ms, wl_main, kt, clocks, launches = timed_value(args.precision, args.steps, args.warmup,
+                                                         True)
+    ms_max = barrier_max(ms)
+    value = world * 1000.0 / ms_max
+
+    # ---- e2e through the public API from pinned host memory ----
+    e2e = None
+    if not args.skip_e2e:
+        host = torch.empty((w.volume * 4 * 18,), dtype=torch.float64, pin_memory=True)
+        hnp = host.numpy().view(np.complex128).reshape(w.volume, 4, 3, 3)
+        ctx.restore()
+        hnp[...] = ctx.download()
+        ctx.upload(hnp)
+        ctx.measure(p)  # warm the staging buffer
+        ext = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize(local)
+        e0.record(ext)
+        for _ in range(args.steps):
+            ctx.upload(hnp)
+            out = ctx.measure(p)
+        e1.record(ext)
+        e1.synchronize()
+        barrier()
+        ems = barrier_max(e0.elapsed_time(e1) / args.steps)
+        e2e = {"value": world * 1000.0 / ems, "unit": UNIT,
+               "h2d_bytes_per_step": int(hnp.nbytes), "d2h_bytes_per_step": int(out.nbytes)}
+    ctx.close()
+
+    # ---- FP64 form and the mixed-vs-FP64 error ----
+    fp64 = None
+    if not args.skip_fp64 and args.precision == "mixed":
+        c64, ms64, wl64, kt64, _, _ = timed_value("fp64", max(2, min(args.steps, 3)), 1, True)
+        c64.close()
+        ms64 = barrier_max(ms64)
+        zero = wl64 == 0.0
+        rel = np.abs(wl_main - wl64)[~zero] / np.abs(wl64)[~zero]
+        fp64 = {"value": world * 1000.0 / ms64, "ms_per_step": ms64,
+                "mixed_over_fp64": ms64 / ms_max,
+                "max_rel_err": float(rel.max()),
+                "frac_entries_le_1e-6": float(np.mean(rel <= 1e-6)),
+                "median_rel_err": float(np.median(rel)),
+                "contract_ms_per_launch": kt64["contract"][0] / max(1, kt64["contract"][1])}
+
+    # ---- roofline of the dominant kernel (contraction) ----
+    c_ms, c_n = kt["contract"]
+    per_launch_ms = c_ms / max(1, c_n)
+    flops_per_launch = fl["contract"] / p.mwlr
+    achieved = flops_per_launch / (per_launch_ms * 1e-3) / 1e12
+    peak = peak_tflops(args.precision, local)
+    traffic = load_traffic().get(args.precision)
+    peaks_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm = None
+    if os.path.exists(peaks_file):
+        with open(peaks_file) as f:
+            hbm = json.load(f).get("hbm_gbs")
+    roof = {"kernel": "k_contract (loop contraction)",
+            "bound": "fp32" if args.precision == "mixed" else "fp64",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_source": "vector FMA probe measured in this run (wlg_peak_flops); "
+                           "MEASURED_PEAKS.json has no CUDA-core peak",
+            "flops_per_launch": flops_per_launch, "ms_per_launch": per_launch_ms,
+            "traffic": traffic}
+    if traffic and hbm:
+        roof["hbm_frac_of_measured"] = traffic / (per_launch_ms * 1e-3) / 1e9 / hbm
+    total_ms = sum(v[0] for v in kt.values())
+    shares = {k: round(v[0] / total_ms, 4) for k, v in kt.items() if total_ms > 0}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        threads = os.cpu_count() or 1
+        v, wall, sample = cpu_sample(16, 32, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+                "data": "synthetic",
+                "config": {"workload": "c3: 32^3x64 periodic, eps 0.2, HYP2 (1,1,0.5) proj 4, "
+                                       "APE 0.5 nss 0 10 10 10 10 10, msl 6, r<=16, t<=24",
+                           "precision": args.precision, "parallelism": f"replicas x{world}",
+                           "l2": "inputs larger than L2 (field 151-302 MB, level store 1.9-3.8 GB)"},
+                "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+                "gpu_launches": launches, "fp64_form": fp64, "kernel_share": shares,
+                "algorithmic_flops_per_config": fl["total"]}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -131,6 +131,17 @@ int wlg_kernel_time(wlg_ctx* ctx, const char* name, double* total_ms, long long*
 int wlg_reset_kernel_times(wlg_ctx* ctx);
 /* Tuning knobs of the contraction kernel (0 = automatic). */
 int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
+/* The context's CUDA stream (cudaStream_t), for callers that record events. */
+void* wlg_stream(wlg_ctx* ctx);
+/* Number of wloop_b200 kernel launches issued by this process so far. */
+long long wlg_launch_count(void);
+/* Keep a device copy of the current gauge field / put it back (device to
+ * device; lets repeated measurements start from the unsmeared field). */
+int wlg_snapshot(wlg_ctx* ctx);
+int wlg_restore(wlg_ctx* ctx);
+/* Achievable vector FMA throughput of the device in TFLOP/s (2 flops per
+ * FMA), FP64 or FP32 (precision WLG_FP64 / WLG_MIXED). */
+int wlg_peak_flops(int precision, int device, double* tflops);
 
 #ifdef __cplusplus
 }

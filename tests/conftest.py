@@ -23,8 +23,8 @@ def pytest_configure(config):
                        capture_output=True)
     lib_so = os.path.join(ROOT, "wloop_b200", "_lib", "libwloop_b200.so")
     if not os.path.exists(lib_so):
-        from wloop_b200.build import build
-        build()
+        subprocess.run([sys.executable, os.path.join(ROOT, "wloop_b200", "build.py")], check=True,
+                       capture_output=True)
 
 
 def _has_gpu():

@@ -1,0 +1,285 @@
+"""GPU parity: the sm_100a kernels against the FP64 oracle, through the C ABI.
+
+FP64 bar: every Wilson-loop entry within 1e-12 relative, measured as
+|W_gpu - W_oracle| <= 1e-12 * max(|W_oracle|, A_oracle) with A the oracle's
+sum of |Re tr| over the averaged terms (entries near zero are limited by
+summation order, not by the kernels); entries that are exactly zero in the
+oracle (loops crossing an open boundary) must be exactly zero.  Smeared
+links and plaquettes: 1e-13 absolute per matrix element / 1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+from tests import lattice_np as L
+from tests import oracle as O
+from wloop_b200 import APE, HYP, Context, WloopParms, approx_project_to_su3, generate_links
+from wloop_b200.api import staple_sum
+
+pytestmark = pytest.mark.gpu
+
+TOL_W = 1e-12
+
+
+def assert_wl_close(got, ref, ref_abs, tol=TOL_W):
+    zero = ref == 0.0
+    assert np.all(got[zero] == 0.0), "exact zeros (open-bc crossing loops) must stay exact"
+    scale = np.maximum(np.abs(ref), ref_abs)
+    err = np.abs(got - ref)[~zero] / scale[~zero]
+    assert err.max() <= tol, f"max scaled error {err.max():.3e}"
+    return err.max()
+
+
+def test_generator_device_equals_host():
+    n, bc = (4, 6, 4, 8), 0
+    host = generate_links(n, bc, 1234, 0.27)
+    with Context(n, bc, "fp64") as c:
+        c.generate(1234, 0.27)
+        dev = c.download()
+    assert np.array_equal(dev.view(np.uint64), host.view(np.uint64))
+
+
+def test_upload_download_roundtrip():
+    n = (4, 4, 6, 4)
+    u = generate_links(n, 3, 5, 0.3)
+    with Context(n, 3, "fp64") as c:
+        c.upload(u)
+        assert np.array_equal(c.download(), u)
+    with Context(n, 3, "mixed") as c:
+        c.upload(u)
+        d = c.download()
+        assert np.abs(d - u).max() < 1e-7
+
+
+def _openqcd_ipt(n):
+    """An openQCD-style ipt[]: even sites first, then odd (lexicographic within)."""
+    x = np.indices(n).reshape(4, -1)
+    par = x.sum(axis=0) % 2
+    ipt = np.empty(x.shape[1], dtype=np.int32)
+    ev = np.nonzero(par == 0)[0]
+    od = np.nonzero(par == 1)[0]
+    ipt[ev] = np.arange(len(ev))
+    ipt[od] = len(ev) + np.arange(len(od))
+    return ipt
+
+
+def _to_openqcd(u, n, ipt):
+    """Host-side packing into the openQCD layout (lnkcom.c:840-859)."""
+    vol = int(np.prod(n))
+    ud = np.zeros((4 * vol, 3, 3), dtype=np.complex128)
+    U = L.as5d(u, n)
+    inv = np.empty(vol, dtype=np.int64)
+    inv[ipt] = np.arange(vol)
+    xs = np.array(np.unravel_index(np.arange(vol), n)).T
+    for iq in range(vol // 2, vol):
+        s = inv[iq]
+        x = xs[s]
+        for mu in range(4):
+            ud[8 * (iq - vol // 2) + 2 * mu] = U[tuple(x)][mu]
+            y = x.copy()
+            y[mu] = (y[mu] - 1) % n[mu]
+            ud[8 * (iq - vol // 2) + 2 * mu + 1] = U[tuple(y)][mu]
+    return ud
+
+
+def test_openqcd_layout():
+    n = (4, 4, 4, 6)
+    u = generate_links(n, 3, 9, 0.3)
+    ipt = _openqcd_ipt(n)
+    ud = _to_openqcd(u, n, ipt)
+    with Context(n, 3, "fp64") as c:
+        c.upload_openqcd(ud, ipt)
+        assert np.array_equal(c.download(), u)
+        back = c.download_openqcd(ipt)
+        assert np.array_equal(back, ud)
+
+
+def test_projection():
+    rng = np.random.default_rng(3)
+    m = (rng.standard_normal((300, 3, 3)) + 1j * rng.standard_normal((300, 3, 3))) * 0.4 + np.eye(3)
+    m[7] = 0.0
+    ref = O.project(m, 6)
+    got = np.ascontiguousarray(m.copy())
+    approx_project_to_su3(got, 6)
+    assert np.all(got[7] == 0.0)
+    assert np.abs(got - ref).max() < 1e-14
+
+
+def test_staple_sum():
+    n = (4, 4, 2, 6)
+    u1 = generate_links(n, 3, 1, 0.3)
+    u2 = generate_links(n, 3, 2, 0.3)
+    vb = generate_links(n, 3, 3, 0.3)
+    for mu, nu in [(0, 2), (3, 1), (1, 0)]:
+        ref = O.staple_sum(n, u1, u2, mu, nu, vb)
+        got = vb.copy()
+        staple_sum(n, u1, u2, mu, nu, got)
+        assert np.abs(got - ref).max() < 1e-14
+
+
+@pytest.mark.parametrize("bc", [0, 3])
+def test_plaquette(bc):
+    n = (6, 4, 4, 8)
+    u = generate_links(n, bc, 17, 0.3)
+    ref = O.plaq_sum(n, bc, u)
+    for prec, tol in [("fp64", 1e-13), ("mixed", 1e-6)]:
+        with Context(n, bc, prec) as c:
+            c.upload(u)
+            assert abs(c.lnk_plaq_sum() - ref) / abs(ref) < tol
+
+
+@pytest.mark.parametrize("bc", [0, 3])
+@pytest.mark.parametrize("mask", ["all", "time", "space"])
+def test_hyp(bc, mask):
+    n = (4, 6, 4, 4)
+    u = generate_links(n, bc, 23, 0.3)
+    t, s = {"all": (1, 1), "time": (1, 0), "space": (0, 1)}[mask]
+    ref = O.hyp_links(n, bc, u, 1.0, 1.0, 0.5, 1, 4, time=t, space=s)
+    with Context(n, bc, "fp64") as c:
+        c.upload(u)
+        {"all": c.hyp_links, "time": c.hyp_time_links, "space": c.hyp_space_links}[mask](
+            1.0, 1.0, 0.5, 1, 4)
+        got = c.download()
+    assert np.abs(got - ref).max() < 1e-13
+
+
+def test_hyp_no_projection_and_skip():
+    n = (4, 4, 4, 4)
+    u = generate_links(n, 3, 29, 0.3)
+    ref = O.hyp_links(n, 3, u, 0.75, 0.6, 0.3, 0, 0)
+    with Context(n, 3, "fp64") as c:
+        c.upload(u)
+        c.hyp_links(0.75, 0.6, 0.3, 0, 0)
+        assert np.abs(c.download() - ref).max() < 1e-13
+        c.upload(u)
+        c.hyp_links(0.0, 0.6, 0.3, 1, 4)  # a1 == 0: no-op (hyp_links.c:405)
+        assert np.array_equal(c.download(), u)
+
+
+@pytest.mark.parametrize("time", [0, 1])
+def test_ape(time):
+    n = (4, 4, 6, 4)
+    u = generate_links(n, 3, 31, 0.3)
+    ref = O.ape_links(n, u, 0.5, 1, 4, time=time, nsweeps=3)
+    with Context(n, 3, "fp64") as c:
+        c.upload(u)
+        (c.ape_links if time else c.ape_spatial_links)(0.5, 1, 4, nsweeps=3)
+        got = c.download()
+    assert np.abs(got - ref).max() < 1e-13
+
+
+def test_hyp_spatial():
+    n = (4, 4, 4, 6)
+    u = generate_links(n, 3, 37, 0.3)
+    ref = O.hyp_spatial_links(n, u, 0.75, 0.3, 1, 4, nsweeps=2)
+    with Context(n, 3, "fp64") as c:
+        c.upload(u)
+        c.hyp_spatial_links(0.75, 0.3, 1, 4, nsweeps=2)
+        got = c.download()
+    assert np.abs(got - ref).max() < 1e-13
+
+
+CASES = [
+    # (n, bc, parms)
+    ((8, 8, 8, 8), 3, WloopParms(msl=4, nss=[0, 5, 5, 5], mwlt=4, mwlr=4, op_smear=APE,
+                                 alpha_ape=0.5, proj_iter=4)),                 # BASELINE c1
+    ((8, 4, 6, 4), 0, WloopParms(msl=3, nss=[0, 2, 2], mwlt=5, mwlr=3, op_smear=APE,
+                                 alpha_ape=0.5, proj_iter=4)),
+    ((6, 4, 4, 4), 3, WloopParms(msl=3, nss=[0, 1, 2], mwlt=4, mwlr=3, op_smear=HYP,
+                                 alpha_hyp=(0.75, 0.3), proj_iter=4)),
+    ((4, 4, 4, 4), 0, WloopParms(msl=5, nss=[0, 1, 0, 1, 1], mwlt=3, mwlr=3, op_smear=APE,
+                                 alpha_ape=0.4, proj_iter=0)),
+    ((10, 6, 6, 6), 0, WloopParms(msl=6, nss=[0, 2, 2, 2, 2, 2], mwlt=6, mwlr=4, op_smear=APE,
+                                  alpha_ape=0.5, proj_iter=4)),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_wloop_sum_fp64(case):
+    n, bc, p = CASES[case]
+    u = generate_links(n, bc, 100 + case, 0.25)
+    uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
+    ref, ref_abs, ref_plaq = O.wloop_sum(n, bc, uh, p, want_abs=True, want_plaq=True)
+    with Context(n, bc, "fp64") as c:
+        c.upload(u)
+        got, plaq = c.measure(p, plaq=True)
+    assert_wl_close(got, ref, ref_abs)
+    assert np.abs(plaq - ref_plaq).max() / np.abs(ref_plaq).max() < 1e-12
+
+
+@pytest.mark.parametrize("case", [0, 1, 4])
+def test_wloop_sum_mixed(case):
+    n, bc, p = CASES[case]
+    u = generate_links(n, bc, 100 + case, 0.25)
+    uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
+    ref, ref_abs = O.wloop_sum(n, bc, uh, p, want_abs=True)
+    with Context(n, bc, "mixed") as c:
+        c.upload(u)
+        got = c.measure(p)
+    zero = ref == 0.0
+    assert np.all(got[zero] == 0.0)
+    rel = np.abs(got - ref)[~zero] / np.abs(ref)[~zero]
+    scaled = np.abs(got - ref)[~zero] / np.maximum(np.abs(ref), ref_abs)[~zero]
+    print(f"mixed vs oracle: max rel {rel.max():.2e}, max scaled {scaled.max():.2e}")
+    assert scaled.max() < 2e-6
+
+
+@pytest.mark.parametrize("bc", [0, 3])
+def test_unit_field(bc):
+    """devel/wloop/check1.c on the GPU (W = 1, crossing loops 0)."""
+    n = (8, 4, 4, 4)
+    p = WloopParms(msl=4, nss=[0, 1, 2, 3], mwlt=4, mwlr=3, op_smear=APE, alpha_ape=0.5,
+                   proj_iter=10)
+    u = L.unit_field(n, bc)
+    with Context(n, bc, "fp64") as c:
+        c.upload(u)
+        c.hyp_time_links(1.0, 1.0, 0.5, 1, 10)
+        wl = c.wloop_sum(p).reshape(n[0], p.mwlr, p.mwlt, p.msl, p.msl)
+    eps = np.sqrt(3.0) * n[0] * n[1] / 4 * np.finfo(float).eps
+    for x0 in range(n[0]):
+        for t in range(p.mwlt):
+            if bc == 0 and x0 + t + 1 > n[0] - 1:
+                assert np.all(wl[x0, :, t] == 0.0)
+            else:
+                assert np.abs(wl[x0, :, t] - 1.0).max() < eps
+
+
+def test_gauge_invariance_gpu():
+    """devel/wloop/check2.c on the GPU at 8^3x16, open bc."""
+    n, bc = (16, 8, 8, 8), 0
+    p = WloopParms(msl=3, nss=[0, 2, 3], mwlt=6, mwlr=4, op_smear=HYP, alpha_hyp=(1.0, 0.5),
+                   proj_iter=0)
+    u = generate_links(n, bc, 77, 0.3)
+    g = L.random_su3(tuple(n), np.random.default_rng(5))
+    ug = L.gauge_transform(u, n, bc, g)
+    with Context(n, bc, "fp64") as c:
+        c.upload(u)
+        w1 = c.measure(p)
+        c.upload(ug)
+        w2 = c.measure(p)
+    eps = 100 * np.sqrt(p.msl ** 2 * p.mwlr * p.mwlt * 3 * np.prod(n)) * np.finfo(float).eps
+    nz = w1 != 0
+    assert np.array_equal(w2 == 0, ~nz)
+    assert np.abs(1.0 - w2[nz] / w1[nz]).max() < eps
+
+
+def test_levels_match_oracle():
+    n, bc = (6, 4, 4, 4), 3
+    p = WloopParms(msl=3, nss=[1, 2, 0], mwlt=2, mwlr=2, op_smear=APE, alpha_ape=0.5, proj_iter=4)
+    u = generate_links(n, bc, 3, 0.3)
+    _, lv = O.wloop_sum(n, bc, u, p, want_levels=True)
+    with Context(n, bc, "fp64") as c:
+        c.upload(u)
+        c.wloop_sum(p)
+        for sl in range(p.msl):
+            assert np.abs(c.level(sl) - lv[sl]).max() < 1e-13
+
+
+def test_parameter_errors():
+    n = (4, 4, 4, 4)
+    with Context(n, 3, "fp64") as c:
+        for p in [WloopParms(msl=9, nss=[0] * 8, mwlt=1, mwlr=1),
+                  WloopParms(msl=1, nss=[0], mwlt=4, mwlr=1),
+                  WloopParms(msl=1, nss=[0], mwlt=1, mwlr=4),
+                  WloopParms(msl=1, nss=[0], mwlt=1, mwlr=1, op_smear=5)]:
+            with pytest.raises(Exception):
+                c.wloop_sum(p)

@@ -1,6 +1,6 @@
 """ctypes binding of libwloop_b200.so (the C ABI in include/wloop_b200.h).
 
-The library is built in-tree by ``python -m wloop_b200.build``.  Importing
+The library is built in-tree by ``python wloop_b200/build.py``.  Importing
 this module without the built library raises: there is no CPU fallback.
 """
 from __future__ import annotations
@@ -41,7 +41,7 @@ def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
             f"wloop_b200: native library {LIB_PATH} is not built; run "
-            "`python -m wloop_b200.build` (the CUDA path has no CPU fallback)")
+            "`python wloop_b200/build.py` (the CUDA path has no CPU fallback)")
     lib = C.CDLL(LIB_PATH, mode=C.RTLD_GLOBAL)
     vp, ip, dp, i, d = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int, C.c_double
     u64, u32 = C.c_uint64, C.c_uint32
@@ -73,6 +73,11 @@ def _load():
         "wlg_kernel_time": (i, [vp, C.c_char_p, dp, C.POINTER(C.c_longlong)]),
         "wlg_reset_kernel_times": (i, [vp]),
         "wlg_set_contract_shape": (i, [vp, i, i, i]),
+        "wlg_stream": (vp, [vp]),
+        "wlg_launch_count": (C.c_longlong, []),
+        "wlg_snapshot": (i, [vp]),
+        "wlg_restore": (i, [vp]),
+        "wlg_peak_flops": (i, [i, i, dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

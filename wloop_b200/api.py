@@ -225,6 +225,27 @@ class Context:
     def set_contract_shape(self, G=0, nCB=0, block=0):
         check(lib.wlg_set_contract_shape(self._h, G, nCB, block), "set_contract_shape")
 
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the context (for event timing by the caller)."""
+        return lib.wlg_stream(self._h) or 0
+
+    def snapshot(self):
+        check(lib.wlg_snapshot(self._h), "snapshot")
+
+    def restore(self):
+        check(lib.wlg_restore(self._h), "restore")
+
+
+def launch_count() -> int:
+    return lib.wlg_launch_count()
+
+
+def peak_tflops(precision: str = "mixed", device: int = 0) -> float:
+    out = np.zeros(1)
+    check(lib.wlg_peak_flops(PRECISIONS[precision], device, dptr(out)), "peak_flops")
+    return float(out[0])
+
 
 def staple_sum(n, u1: np.ndarray, u2: np.ndarray, mu: int, nu: int, vb: np.ndarray) -> None:
     """staple_sum (staple_sum.c:53-87) on AoS host fields; vb is updated."""

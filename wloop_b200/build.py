@@ -1,6 +1,7 @@
 """Builds libwloop_b200.so in-tree for sm_100a.
 
-Usage: python -m wloop_b200.build [--force]
+Usage: python wloop_b200/build.py [--force]   (a plain script: importing the
+package itself would load the library being built)
 
 Every .cu file is compiled by nvcc with -gencode arch=compute_100a,code=sm_100a;
 gen_dev.cu is compiled with --fmad=false and gen_host.cpp with

@@ -4,6 +4,7 @@
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
+#include <atomic>
 #include <map>
 #include <string>
 #include <vector>
@@ -21,6 +22,9 @@ void set_error(const char* fmt, ...) {
   va_end(ap);
 }
 const char* get_error() { return g_err; }
+
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int num_sms() {
   static int cached[64] = {0};
@@ -54,7 +58,7 @@ struct wlg_ctx {
   int dev = 0, prec = WLG_FP64, bc = 3;
   Geo g;
   cudaStream_t st = nullptr;
-  DevBuf U, bar, til, apeA, apeB, dl, levels, lines, partial, wl, plaq_part, plaq_out, staging, ipt;
+  DevBuf U, U0, bar, til, apeA, apeB, dl, levels, lines, partial, wl, plaq_part, plaq_out, staging, ipt;
   int cG = 0, cNCB = 0, cBlock = 0;
   bool prof = false;
   std::map<std::string, ProfStat> stats;
@@ -460,7 +464,7 @@ int wlg_destroy(wlg_ctx* c) {
   cudaSetDevice(c->dev);
   cudaStreamSynchronize(c->st);
   harvest(c);
-  DevBuf* all[] = {&c->U, &c->bar, &c->til, &c->apeA, &c->apeB, &c->dl, &c->levels, &c->lines,
+  DevBuf* all[] = {&c->U, &c->U0, &c->bar, &c->til, &c->apeA, &c->apeB, &c->dl, &c->levels, &c->lines,
                    &c->partial, &c->wl, &c->plaq_part, &c->plaq_out, &c->staging, &c->ipt};
   for (DevBuf* b : all) release(*b);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
@@ -501,8 +505,32 @@ int wlg_download_links(wlg_ctx* c, double* aos) {
   return finish("download_links");
 }
 
+// ipt must be a permutation of [0,V) that puts even sites first: it is used
+// as an index on the device, so it is checked here.
+static int check_ipt(const wlg_ctx* c, const int* ipt) {
+  if (!ipt) {
+    set_error("null ipt");
+    return -1;
+  }
+  const Geo& g = c->g;
+  std::vector<char> seen(g.vol, 0);
+  for (int s = 0; s < g.vol; s++) {
+    int iq = ipt[s];
+    int x0 = s / g.st[0], r = s % g.st[0];
+    int x1 = r / g.st[1], x2 = (r % g.st[1]) / g.st[2], x3 = r % g.st[2];
+    int even = ((x0 + x1 + x2 + x3) & 1) == 0;
+    if (iq < 0 || iq >= g.vol || seen[iq] || (even != (iq < g.vol / 2))) {
+      set_error("ipt[%d]=%d is not an even-first permutation of the %d sites", s, iq, g.vol);
+      return -1;
+    }
+    seen[iq] = 1;
+  }
+  return 0;
+}
+
 int wlg_upload_openqcd(wlg_ctx* c, const double* ud, const int* ipt) {
   CTX_BEGIN(c);
+  if (check_ipt(c, ipt)) return -1;
   size_t bytes = (size_t)4 * 144 * c->g.vol;
   if (ensure(c->staging, bytes) || ensure(c->ipt, sizeof(int) * c->g.vol)) return -1;
   WLG_CUDA(cudaMemcpyAsync(c->staging.p, ud, bytes, cudaMemcpyHostToDevice, c->st));
@@ -519,6 +547,7 @@ int wlg_upload_openqcd(wlg_ctx* c, const double* ud, const int* ipt) {
 
 int wlg_download_openqcd(wlg_ctx* c, double* ud, const int* ipt) {
   CTX_BEGIN(c);
+  if (check_ipt(c, ipt)) return -1;
   size_t bytes = (size_t)4 * 144 * c->g.vol;
   if (ensure(c->staging, bytes) || ensure(c->ipt, sizeof(int) * c->g.vol)) return -1;
   WLG_CUDA(cudaMemcpyAsync(c->ipt.p, ipt, sizeof(int) * c->g.vol, cudaMemcpyHostToDevice, c->st));
@@ -706,4 +735,78 @@ int wlg_set_contract_shape(wlg_ctx* c, int G, int nCB, int block) {
   return 0;
 }
 
+void* wlg_stream(wlg_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+long long wlg_launch_count(void) { return g_launches.load(); }
+
+int wlg_snapshot(wlg_ctx* c) {
+  CTX_BEGIN(c);
+  if (ensure(c->U0, field_bytes(c, 4))) return -1;
+  WLG_CUDA(cudaMemcpyAsync(c->U0.p, c->U.p, field_bytes(c, 4), cudaMemcpyDeviceToDevice, c->st));
+  return finish("snapshot");
+}
+
+int wlg_restore(wlg_ctx* c) {
+  CTX_BEGIN(c);
+  if (!c->U0.p) {
+    set_error("restore: no snapshot");
+    return -1;
+  }
+  WLG_CUDA(cudaMemcpyAsync(c->U.p, c->U0.p, field_bytes(c, 4), cudaMemcpyDeviceToDevice, c->st));
+  return finish("restore");
+}
+
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// vector FMA throughput probe: 8 independent FMA chains per thread
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_peak(T* out, int iters, T a, T b) {
+  T x[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) x[j] = (T)(threadIdx.x + j) * (T)1e-3;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) x[j] = fma(x[j], a, b);
+  }
+  T s = 0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) s += x[j];
+  if (s == (T)-12345.0) out[threadIdx.x] = s;  // keeps the chains live
+}
+
+template <class T> static int peak_impl(int device, double* tflops) {
+  WLG_CUDA(cudaSetDevice(device));
+  T* out = nullptr;
+  WLG_CUDA(cudaMalloc(&out, 256 * sizeof(T)));
+  int blocks = num_sms() * 8, iters = 1 << 15;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(a);
+    k_peak<T><<<blocks, 256>>>(out, iters, (T)0.999, (T)1e-4);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (rep > 0 && ms < best) best = ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  double flops = 2.0 * 8.0 * iters * 256.0 * blocks;
+  *tflops = flops / (best * 1e-3) / 1e12;
+  return finish("peak_flops");
+}
+
+extern "C" int wlg_peak_flops(int precision, int device, double* tflops) {
+  set_error("%s", "");
+  if (wlg_device_count() <= 0) {
+    set_error("no CUDA device");
+    return -1;
+  }
+  return precision == WLG_FP64 ? peak_impl<double>(device, tflops) : peak_impl<float>(device, tflops);
+}

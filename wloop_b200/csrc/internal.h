@@ -100,9 +100,10 @@ void convert(typename V2<D>::t* dst, const typename V2<S>::t* src, size_t n, cud
 template <class T>
 void generate_soa(const Geo& g, int bc, uint64_t seed, double eps, Links<T> U, cudaStream_t st);
 
-// ---- error handling -------------------------------------------------------
+// ---- error handling and launch accounting ---------------------------------
 void set_error(const char* fmt, ...);
 const char* get_error();
+void count_launch();
 
 }  // namespace wlg
 
@@ -118,6 +119,7 @@ const char* get_error();
 
 #define WLG_LAUNCH_CHECK(name)                                                            \
   do {                                                                                    \
+    wlg::count_launch();                                                                  \
     cudaError_t e_ = cudaGetLastError();                                                  \
     if (e_ != cudaSuccess) {                                                              \
       wlg::set_error("kernel %s: %s", name, cudaGetErrorString(e_));                      \
