@@ -112,9 +112,14 @@ int wlg_wloop_sum(wlg_ctx* ctx, const wlg_wloop_parms* p, double* wl_mat, double
 /* HYP (alpha_action, all directions, as ms10 set_data does: main/ms10.c:633-646)
  * followed by wlg_wloop_sum. */
 int wlg_measure(wlg_ctx* ctx, const wlg_wloop_parms* p, double* wl_mat, double* plaq);
-/* Level store after wlg_wloop_sum: spatial links of level sl in AoS
- * [V][3][18] (get_pus, smear.c:124-127). */
+/* Only the smearing levels of wlg_wloop_sum (smear(), smear.c:99-121). */
+int wlg_smear_levels(wlg_ctx* ctx, const wlg_wloop_parms* p, double* plaq);
+/* Level store after wlg_smear_levels / wlg_wloop_sum: spatial links of
+ * level sl in AoS [V][3][18] (get_pus slots 0..msl-1, smear.c:124-127). */
 int wlg_download_level(wlg_ctx* ctx, int sl, double* aos3);
+/* Spatial lines of level sl left by the last wlg_wloop_sum (length *length
+ * = mwlr >= 2; get_pus slots msl..2msl-1 after wloops). */
+int wlg_download_lines(wlg_ctx* ctx, int sl, double* aos3, int* length);
 
 /* ---- single-field kernels of the lnk/smear API ------------------------------
  * vb(x,mu) += staples of the (mu,nu) plane, nu-links from u1, mu-links from
@@ -129,8 +134,13 @@ int wlg_set_profiling(wlg_ctx* ctx, int on);
 /* name: "hyp", "ape", "plaq", "lines", "contract", "reduce" */
 int wlg_kernel_time(wlg_ctx* ctx, const char* name, double* total_ms, long long* launches);
 int wlg_reset_kernel_times(wlg_ctx* ctx);
-/* Tuning knobs of the contraction kernel (0 = automatic). */
+/* Tuning knobs of the contraction kernel (0 = automatic): G bottom levels
+ * per thread (1,2,3,4,6), nCB column blocks per (x0, level group), block
+ * threads (multiple of 32, at most 128). */
 int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
+/* As above plus the kernel form (1 or 2) and SB top levels per reduction
+ * (1 or 2). */
+int wlg_set_contract_tuning(wlg_ctx* ctx, int variant, int G, int SB, int nCB, int block);
 /* The context's CUDA stream (cudaStream_t), for callers that record events. */
 void* wlg_stream(wlg_ctx* ctx);
 /* Number of wloop_b200 kernel launches issued by this process so far. */

@@ -73,6 +73,7 @@ def _load():
         "wlg_kernel_time": (i, [vp, C.c_char_p, dp, C.POINTER(C.c_longlong)]),
         "wlg_reset_kernel_times": (i, [vp]),
         "wlg_set_contract_shape": (i, [vp, i, i, i]),
+        "wlg_set_contract_tuning": (i, [vp, i, i, i, i, i]),
         "wlg_stream": (vp, [vp]),
         "wlg_launch_count": (C.c_longlong, []),
         "wlg_snapshot": (i, [vp]),

@@ -225,6 +225,10 @@ class Context:
     def set_contract_shape(self, G=0, nCB=0, block=0):
         check(lib.wlg_set_contract_shape(self._h, G, nCB, block), "set_contract_shape")
 
+    def set_contract_tuning(self, variant=0, G=0, SB=0, nCB=0, block=0):
+        check(lib.wlg_set_contract_tuning(self._h, variant, G, SB, nCB, block),
+              "set_contract_tuning")
+
     @property
     def stream(self) -> int:
         """cudaStream_t of the context (for event timing by the caller)."""

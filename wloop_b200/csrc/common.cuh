@@ -1,11 +1,16 @@
 // common.cuh -- device types shared by every wloop_b200 kernel.
 //
-// Link fields live in HBM as structure-of-arrays: for direction mu, complex
-// component c (row-major c11..c33 -> 0..8) and lexicographic site s
-//     field[(mu*9 + c)*vol + s]          (double2 in FP64, float2 in mixed)
-// so a warp reading component c of 32 consecutive sites issues one fully
-// coalesced 512 B (FP64) or 256 B (FP32) request.  The site index is
-// s = x3 + N3*(x2 + N2*(x1 + N1*x0)), the argument order of openQCD's ipt[].
+// Link fields live in HBM in a tiled structure-of-arrays layout: each
+// direction of a field is an array of 32-site tiles (lexicographic site
+// s = x3 + N3*(x2 + N2*(x1 + N1*x0)), the argument order of openQCD's
+// ipt[]); a tile holds the 9 complex entries (row-major c11..c33) of its 32
+// links component-major, so a warp reading one component of 32 consecutive
+// sites issues one fully coalesced request and the 9 components of a link
+// sit at compile-time offsets from one base address.
+//   FP64: component c of site s at double2 index  (s/32)*288 + c*32 + s%32
+//   FP32: entries paired into float4 (c = 2p, 2p+1; p = 0..4, the 10th slot
+//         is padding) at float4 index  (s/32)*160 + p*32 + s%32
+// so FP64 links load as 9 and FP32 links as 5 128-bit transactions.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -77,18 +82,59 @@ template <class T> struct Links {
   typename V2<T>::t* p[4];
 };
 
-template <class T>
-__device__ __forceinline__ void ld(M3<T>& m, const typename V2<T>::t* __restrict__ base, int vol,
-                                   int s) {
-#pragma unroll
-  for (int c = 0; c < 9; c++) m.e[c] = __ldg(base + (size_t)c * vol + s);
+// elements (of V2<T>::t) per 32-site tile and per direction array
+template <class T> struct Tile;
+template <> struct Tile<double> { enum { TS = 288 }; };  // 9 x 32 double2
+template <> struct Tile<float> { enum { TS = 320 }; };   // 5 x 32 float4 = 320 float2
+template <class T> __host__ __device__ __forceinline__ size_t link_elems(int vol) {
+  return (size_t)((vol + 31) >> 5) * Tile<T>::TS;
 }
 
 template <class T>
+__device__ __forceinline__ void ld(M3<T>& m, const typename V2<T>::t* __restrict__ base, int vol,
+                                   int s);
+template <class T>
 __device__ __forceinline__ void st(typename V2<T>::t* __restrict__ base, int vol, int s,
-                                   const M3<T>& m) {
+                                   const M3<T>& m);
+
+template <>
+__device__ __forceinline__ void ld<double>(M3<double>& m, const double2* __restrict__ base, int,
+                                           int s) {
+  const double2* p = base + (size_t)(s >> 5) * 288 + (s & 31);
 #pragma unroll
-  for (int c = 0; c < 9; c++) base[(size_t)c * vol + s] = m.e[c];
+  for (int c = 0; c < 9; c++) m.e[c] = __ldg(p + c * 32);
+}
+template <>
+__device__ __forceinline__ void st<double>(double2* __restrict__ base, int, int s,
+                                           const M3<double>& m) {
+  double2* p = base + (size_t)(s >> 5) * 288 + (s & 31);
+#pragma unroll
+  for (int c = 0; c < 9; c++) p[c * 32] = m.e[c];
+}
+template <>
+__device__ __forceinline__ void ld<float>(M3<float>& m, const float2* __restrict__ base, int,
+                                          int s) {
+  const float4* p = reinterpret_cast<const float4*>(base) + (size_t)(s >> 5) * 160 + (s & 31);
+#pragma unroll
+  for (int q = 0; q < 5; q++) {
+    float4 v = __ldg(p + q * 32);
+    m.e[2 * q] = make_float2(v.x, v.y);
+    if (q < 4) m.e[2 * q + 1] = make_float2(v.z, v.w);
+  }
+}
+template <>
+__device__ __forceinline__ void st<float>(float2* __restrict__ base, int, int s,
+                                          const M3<float>& m) {
+  float4* p = reinterpret_cast<float4*>(base) + (size_t)(s >> 5) * 160 + (s & 31);
+#pragma unroll
+  for (int q = 0; q < 5; q++) {
+    float4 v;
+    v.x = m.e[2 * q].x;
+    v.y = m.e[2 * q].y;
+    v.z = (q < 4) ? m.e[2 * q + 1].x : 0.f;
+    v.w = (q < 4) ? m.e[2 * q + 1].y : 0.f;
+    p[q * 32] = v;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -162,6 +208,107 @@ template <class T> __device__ __forceinline__ void mul_ad(M3<T>& c, const M3<T>&
     }
 }
 
+// In-place products with 6 temporaries: c <- a^dag c (column by column) and
+// c <- c b (row by row).  Same arithmetic as mul_da / mul.
+template <class T> __device__ __forceinline__ void lmul_dag_inplace(M3<T>& c, const M3<T>& a) {
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    typename V2<T>::t x0 = c.e[j], x1 = c.e[3 + j], x2 = c.e[6 + j];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      T re = a.e[i].x * x0.x + a.e[i].y * x0.y;
+      T im = a.e[i].x * x0.y - a.e[i].y * x0.x;
+      re = fma(a.e[3 + i].x, x1.x, re);
+      re = fma(a.e[3 + i].y, x1.y, re);
+      im = fma(a.e[3 + i].x, x1.y, im);
+      im = fma(-a.e[3 + i].y, x1.x, im);
+      re = fma(a.e[6 + i].x, x2.x, re);
+      re = fma(a.e[6 + i].y, x2.y, re);
+      im = fma(a.e[6 + i].x, x2.y, im);
+      im = fma(-a.e[6 + i].y, x2.x, im);
+      c.e[3 * i + j].x = re;
+      c.e[3 * i + j].y = im;
+    }
+  }
+}
+
+template <class T> __device__ __forceinline__ void rmul_inplace(M3<T>& c, const M3<T>& b) {
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    typename V2<T>::t x0 = c.e[3 * i], x1 = c.e[3 * i + 1], x2 = c.e[3 * i + 2];
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      T re = x0.x * b.e[j].x - x0.y * b.e[j].y;
+      T im = x0.x * b.e[j].y + x0.y * b.e[j].x;
+      re = fma(x1.x, b.e[3 + j].x, re);
+      re = fma(-x1.y, b.e[3 + j].y, re);
+      im = fma(x1.x, b.e[3 + j].y, im);
+      im = fma(x1.y, b.e[3 + j].x, im);
+      re = fma(x2.x, b.e[6 + j].x, re);
+      re = fma(-x2.y, b.e[6 + j].y, re);
+      im = fma(x2.x, b.e[6 + j].y, im);
+      im = fma(x2.y, b.e[6 + j].x, im);
+      c.e[3 * i + j].x = re;
+      c.e[3 * i + j].y = im;
+    }
+  }
+}
+
+// FP32 forms on the packed FP32x2 FMA of sm_100 (__ffma2_rn): a complex
+// multiply-accumulate x*y is (x.re,x.re)*(y.re,y.im) + (x.im,x.im)*(-y.im,y.re),
+// i.e. two packed FMAs instead of four scalar ones.
+__device__ __forceinline__ float2 pk(float a, float b) { return make_float2(a, b); }
+
+template <> __device__ __forceinline__ void lmul_dag_inplace<float>(M3<float>& c, const M3<float>& a) {
+  // out[i][j] = sum_k conj(a[k][i]) c[k][j];
+  // conj(a) x = (a.x,a.x)*(x.x,x.y) + (a.y,-a.y)*(x.y,x.x)
+  float2 ax[9], ay[9];
+#pragma unroll
+  for (int t = 0; t < 9; t++) {
+    ax[t] = pk(a.e[t].x, a.e[t].x);
+    ay[t] = pk(a.e[t].y, -a.e[t].y);
+  }
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const float2 x0 = c.e[j], x1 = c.e[3 + j], x2 = c.e[6 + j];
+    const float2 s0 = pk(x0.y, x0.x), s1 = pk(x1.y, x1.x), s2 = pk(x2.y, x2.x);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      float2 o = __fmul2_rn(ax[i], x0);
+      o = __ffma2_rn(ay[i], s0, o);
+      o = __ffma2_rn(ax[3 + i], x1, o);
+      o = __ffma2_rn(ay[3 + i], s1, o);
+      o = __ffma2_rn(ax[6 + i], x2, o);
+      o = __ffma2_rn(ay[6 + i], s2, o);
+      c.e[3 * i + j] = o;
+    }
+  }
+}
+
+template <> __device__ __forceinline__ void rmul_inplace<float>(M3<float>& c, const M3<float>& b) {
+  // out[i][j] = sum_k c[i][k] b[k][j];  x b = (x.x,x.x)*b + (x.y,x.y)*(-b.y,b.x)
+  float2 bp[9];
+#pragma unroll
+  for (int t = 0; t < 9; t++) bp[t] = pk(-b.e[t].y, b.e[t].x);
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const float2 x0 = c.e[3 * i], x1 = c.e[3 * i + 1], x2 = c.e[3 * i + 2];
+    const float2 r0 = pk(x0.x, x0.x), i0 = pk(x0.y, x0.y);
+    const float2 r1 = pk(x1.x, x1.x), i1 = pk(x1.y, x1.y);
+    const float2 r2 = pk(x2.x, x2.x), i2 = pk(x2.y, x2.y);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      float2 o = __fmul2_rn(r0, b.e[j]);
+      o = __ffma2_rn(i0, bp[j], o);
+      o = __ffma2_rn(r1, b.e[3 + j], o);
+      o = __ffma2_rn(i1, bp[3 + j], o);
+      o = __ffma2_rn(r2, b.e[6 + j], o);
+      o = __ffma2_rn(i2, bp[6 + j], o);
+      c.e[3 * i + j] = o;
+    }
+  }
+}
+
 template <class T> __device__ __forceinline__ void acc(M3<T>& c, const M3<T>& a) {
 #pragma unroll
   for (int k = 0; k < 9; k++) {
@@ -180,6 +327,14 @@ template <class T> __device__ __forceinline__ T retr_dag(const M3<T>& a, const M
     s = fma(a.e[k].y, b.e[k].y, s);
   }
   return s;
+}
+
+// FP32: (sum a.x b.x, sum a.y b.y) in one packed accumulator
+template <> __device__ __forceinline__ float retr_dag<float>(const M3<float>& a, const M3<float>& b) {
+  float2 s = __fmul2_rn(a.e[0], b.e[0]);
+#pragma unroll
+  for (int k = 1; k < 9; k++) s = __ffma2_rn(a.e[k], b.e[k], s);
+  return s.x + s.y;
 }
 
 template <class D, class S> __device__ __forceinline__ void cvt(M3<D>& d, const M3<S>& s) {

@@ -59,7 +59,7 @@ struct wlg_ctx {
   Geo g;
   cudaStream_t st = nullptr;
   DevBuf U, U0, bar, til, apeA, apeB, dl, levels, lines, partial, wl, plaq_part, plaq_out, staging, ipt;
-  int cG = 0, cNCB = 0, cBlock = 0;
+  int cG = 0, cNCB = 0, cBlock = 0, cVariant = 0, cSB = 0;
   bool prof = false;
   std::map<std::string, ProfStat> stats;
   struct Pending {
@@ -69,6 +69,7 @@ struct wlg_ctx {
   std::vector<Pending> pending;
   std::vector<cudaEvent_t> evpool;
   int last_msl = 0;
+  int lines_len = 0;
 };
 
 static int ensure(DevBuf& b, size_t bytes) {
@@ -93,15 +94,17 @@ static void release(DevBuf& b) {
   b.cap = 0;
 }
 
-static size_t link_bytes(const wlg_ctx* c) { return c->prec == WLG_FP64 ? 16 * 9 : 8 * 9; }
-static size_t field_bytes(const wlg_ctx* c, int ndir) {
-  return (size_t)ndir * link_bytes(c) * (size_t)c->g.vol;
+// bytes of one direction array (tiled layout, common.cuh) and of ndir of them
+static size_t dir_bytes(const wlg_ctx* c) {
+  return c->prec == WLG_FP64 ? link_elems<double>(c->g.vol) * sizeof(double2)
+                             : link_elems<float>(c->g.vol) * sizeof(float2);
 }
+static size_t field_bytes(const wlg_ctx* c, int ndir) { return (size_t)ndir * dir_bytes(c); }
 
 template <class T> static Links<T> view4(void* base, int vol) {
   Links<T> L;
   typename V2<T>::t* b = (typename V2<T>::t*)base;
-  for (int mu = 0; mu < 4; mu++) L.p[mu] = b ? b + (size_t)mu * 9 * vol : nullptr;
+  for (int mu = 0; mu < 4; mu++) L.p[mu] = b ? b + (size_t)mu * link_elems<T>(vol) : nullptr;
   return L;
 }
 // spatial-only field stored as 3 directions: p[0] is null
@@ -109,7 +112,7 @@ template <class T> static Links<T> view3(void* base, int vol) {
   Links<T> L;
   typename V2<T>::t* b = (typename V2<T>::t*)base;
   L.p[0] = nullptr;
-  for (int k = 1; k < 4; k++) L.p[k] = b + (size_t)(k - 1) * 9 * vol;
+  for (int k = 1; k < 4; k++) L.p[k] = b + (size_t)(k - 1) * link_elems<T>(vol);
   return L;
 }
 
@@ -219,7 +222,7 @@ template <class T> static int do_ape(wlg_ctx* c, double alpha, int proj, int pit
     }
   }
   if (nsweeps % 2 == 1) {
-    size_t off = (size_t)mu0 * link_bytes(c) * c->g.vol;
+    size_t off = (size_t)mu0 * dir_bytes(c);
     WLG_CUDA(cudaMemcpyAsync((char*)c->U.p + off, (char*)c->apeA.p + off,
                              field_bytes(c, 4 - mu0), cudaMemcpyDeviceToDevice, c->st));
   }
@@ -239,7 +242,7 @@ template <class T> static int hyp3_sweep(wlg_ctx* c, Links<T> src, Links<T> dst,
   if (src.p[1] != dst.p[1]) {
     // level 2 reads only its own src link for the linear combination
     for (int k = 1; k < 4; k++)
-      WLG_CUDA(cudaMemcpyAsync(dst.p[k], src.p[k], link_bytes(c) * c->g.vol,
+      WLG_CUDA(cudaMemcpyAsync(dst.p[k], src.p[k], dir_bytes(c),
                                cudaMemcpyDeviceToDevice, c->st));
   }
   hyp3d_level2<T>(c->g, dst, (const typename V2<T>::t*)c->dl.p, a1, proj, piter, c->st);
@@ -298,8 +301,9 @@ static int check_parms(const wlg_ctx* c, const wlg_wloop_parms* p) {
   return 0;
 }
 
+// smear(): spatial smearing levels into the level store (smear.c:99-121)
 template <class T>
-static int do_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, double* plaq) {
+static int do_smear(wlg_ctx* c, const wlg_wloop_parms* p, double* plaq) {
   if (check_parms(c, p)) return -1;
   const Geo& g = c->g;
   const int msl = p->msl, proj = p->proj_iter > 0;
@@ -307,20 +311,16 @@ static int do_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, do
   if (ensure(c->levels, f3 * msl) || ensure(c->apeA, f3) || ensure(c->apeB, f3)) return -1;
   if (ensure(c->plaq_out, sizeof(double) * WLG_MAX_SM_LEVELS)) return -1;
   c->last_msl = msl;
-  typedef typename V2<T>::t T2;
   Links<T> U = view4<T>(c->U.p, g.vol);
   Links<T> A = view3<T>(c->apeA.p, g.vol), B = view3<T>(c->apeB.p, g.vol);
-  auto level = [&](int sl) { return view3<T>((char*)c->levels.p + f3 * sl, g.vol); };
-
-  // ---- smear(): spatial levels (smear.c:99-121) ----
   Links<T> cur = U;
   for (int sl = 0; sl < msl; sl++) {
-    Links<T> lv = level(sl);
+    Links<T> lv = view3<T>((char*)c->levels.p + f3 * sl, g.vol);
     int ns = p->nss[sl];
     if (ns == 0) {
-      WLG_CUDA(cudaMemcpyAsync(lv.p[1], cur.p[1], link_bytes(c) * g.vol, cudaMemcpyDeviceToDevice, c->st));
-      WLG_CUDA(cudaMemcpyAsync(lv.p[2], cur.p[2], link_bytes(c) * g.vol, cudaMemcpyDeviceToDevice, c->st));
-      WLG_CUDA(cudaMemcpyAsync(lv.p[3], cur.p[3], link_bytes(c) * g.vol, cudaMemcpyDeviceToDevice, c->st));
+      for (int k = 1; k < 4; k++)
+        WLG_CUDA(cudaMemcpyAsync(lv.p[k], cur.p[k], dir_bytes(c),
+                                 cudaMemcpyDeviceToDevice, c->st));
     }
     for (int i = 0; i < ns; i++) {
       Links<T> dst = (i == ns - 1) ? lv : ((cur.p[1] == A.p[1]) ? B : A);
@@ -338,13 +338,28 @@ static int do_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, do
       if (do_plaq<T>(c, pl, (double*)c->plaq_out.p + sl)) return -1;
     }
   }
+  if (plaq)
+    WLG_CUDA(cudaMemcpyAsync(plaq, c->plaq_out.p, sizeof(double) * msl, cudaMemcpyDeviceToHost, c->st));
+  return 0;
+}
 
-  // ---- wloops (wloop.c:524-608) ----
+// wloops(): spatial lines, fused temporal lines + contraction, reduction
+// (wloop.c:524-608); needs the level store of do_smear.
+template <class T>
+static int do_loops(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
+  typedef typename V2<T>::t T2;
+  const Geo& g = c->g;
+  const int msl = p->msl;
+  const size_t f3 = field_bytes(c, 3);
+  Links<T> U = view4<T>(c->U.p, g.vol);
   ContractPlan cp = contract_plan(g, msl, p->mwlt, c->prec == WLG_FP64, c->cG, c->cNCB, c->cBlock);
+  if (c->cVariant) cp.variant = c->cVariant;
+  if (c->cSB) cp.SB = c->cSB;
   size_t nwl = (size_t)msl * msl * p->mwlt * p->mwlr * g.n[0];
   if (ensure(c->partial, sizeof(double) * cp.partial_doubles) || ensure(c->wl, sizeof(double) * nwl))
     return -1;
   if (p->mwlr > 1 && ensure(c->lines, f3 * msl)) return -1;
+  c->lines_len = 0;
   const T2* lev = (const T2*)c->levels.p;
   T2* lines = (T2*)c->lines.p;
   for (int r = 0; r < p->mwlr; r++) {
@@ -354,6 +369,7 @@ static int do_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, do
       ProfScope ps(c, "lines");
       line_step<T>(g, msl, R, lev, R == 2 ? lev : lines, lines, c->st);
       L = lines;
+      c->lines_len = R;
     }
     {
       ProfScope ps(c, "contract");
@@ -367,8 +383,12 @@ static int do_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, do
   }
   if (wl_mat)
     WLG_CUDA(cudaMemcpyAsync(wl_mat, c->wl.p, sizeof(double) * nwl, cudaMemcpyDeviceToHost, c->st));
-  if (plaq)
-    WLG_CUDA(cudaMemcpyAsync(plaq, c->plaq_out.p, sizeof(double) * msl, cudaMemcpyDeviceToHost, c->st));
+  return 0;
+}
+
+template <class T>
+static int do_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, double* plaq) {
+  if (do_smear<T>(c, p, plaq) || do_loops<T>(c, p, wl_mat)) return -1;
   WLG_CUDA(cudaStreamSynchronize(c->st));
   return finish("wloop_sum");
 }
@@ -614,6 +634,14 @@ int wlg_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, double* 
                              : do_wloop_sum<float>(c, p, wl_mat, plaq);
 }
 
+int wlg_smear_levels(wlg_ctx* c, const wlg_wloop_parms* p, double* plaq) {
+  CTX_BEGIN(c);
+  int rc = c->prec == WLG_FP64 ? do_smear<double>(c, p, plaq) : do_smear<float>(c, p, plaq);
+  if (rc) return rc;
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  return finish("smear_levels");
+}
+
 int wlg_measure(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, double* plaq) {
   CTX_BEGIN(c);
   if (check_parms(c, p)) return -1;
@@ -624,17 +652,31 @@ int wlg_measure(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, double* pl
   return wlg_wloop_sum(c, p, wl_mat, plaq);
 }
 
+static int download_spatial(wlg_ctx* c, void* base, double* aos3);
+
 int wlg_download_level(wlg_ctx* c, int sl, double* aos3) {
   CTX_BEGIN(c);
   if (!c->levels.p || sl < 0 || sl >= c->last_msl) {
     set_error("level %d not available", sl);
     return -1;
   }
+  return download_spatial(c, (char*)c->levels.p + field_bytes(c, 3) * sl, aos3);
+}
+
+int wlg_download_lines(wlg_ctx* c, int sl, double* aos3, int* length) {
+  CTX_BEGIN(c);
+  if (length) *length = c->lines_len;
+  if (!c->lines.p || c->lines_len < 2 || sl < 0 || sl >= c->last_msl) {
+    set_error("no spatial lines of level %d", sl);
+    return -1;
+  }
+  return download_spatial(c, (char*)c->lines.p + field_bytes(c, 3) * sl, aos3);
+}
+
+static int download_spatial(wlg_ctx* c, void* base, double* aos3) {
   size_t bytes = (size_t)4 * 144 * c->g.vol;
   if (ensure(c->staging, bytes)) return -1;
   // convert to a 4-direction AoS with the temporal slot unused, then compact
-  size_t f3 = field_bytes(c, 3);
-  void* base = (char*)c->levels.p + f3 * sl;
   if (c->prec == WLG_FP64) {
     Links<double> L = view3<double>(base, c->g.vol);
     soa_to_aos<double>(c->g, L, (double*)c->staging.p, 1, 4, c->st);
@@ -723,9 +765,25 @@ int wlg_reset_kernel_times(wlg_ctx* c) {
   return 0;
 }
 
+int wlg_set_contract_tuning(wlg_ctx* c, int variant, int G, int SB, int nCB, int block) {
+  CTX_BEGIN(c);
+  if (variant < 0 || variant > 3 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 || nCB < 0 ||
+      (block != 0 && (block % 32 != 0 || block > 128)) || (variant == 2 && G == 6 && SB == 2)) {
+    set_error("bad contraction tuning (variant %d, G %d, SB %d, nCB %d, block %d)", variant, G,
+              SB, nCB, block);
+    return -1;
+  }
+  c->cVariant = variant;
+  c->cG = G;
+  c->cSB = SB;
+  c->cNCB = nCB;
+  c->cBlock = block;
+  return 0;
+}
+
 int wlg_set_contract_shape(wlg_ctx* c, int G, int nCB, int block) {
   CTX_BEGIN(c);
-  if (G < 0 || G > 6 || nCB < 0 || (block != 0 && (block % 32 != 0 || block > 1024))) {
+  if (G < 0 || G == 5 || G > 6 || nCB < 0 || (block != 0 && (block % 32 != 0 || block > 128))) {
     set_error("bad contraction shape");
     return -1;
   }

@@ -17,12 +17,12 @@ __global__ void k_generate(Geo g, int bc, uint64_t seed, double eps, Links<T> U)
     } else {
       wlg_gen::make_link(seed, (uint64_t)w, eps, v);
     }
+    M3<T> m;
     for (int c = 0; c < 9; c++) {
-      typename V2<T>::t o;
-      o.x = (T)v[2 * c];
-      o.y = (T)v[2 * c + 1];
-      U.p[mu][(size_t)c * g.vol + s] = o;
+      m.e[c].x = (T)v[2 * c];
+      m.e[c].y = (T)v[2 * c + 1];
     }
+    st(U.p[mu], g.vol, s, m);
   }
 }
 

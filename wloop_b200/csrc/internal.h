@@ -60,6 +60,8 @@ void line_step(const Geo& g, int msl, int R, const typename V2<T>::t* level,
 // Contraction for one spatial extent R: partial sums of
 // Re tr(line_s2(x0+T)^dag  U0^dag...  line_s1(x0) ...U0') over columns.
 struct ContractPlan {
+  int variant;  // 1: first form, 2: in-place / prefetching form
+  int SB;       // top levels per shuffle reduction (form 2)
   int G;        // bottom levels per thread
   int ngrp;     // ceil(msl/G)
   int nCB;      // column blocks per (x0, group)
@@ -91,9 +93,6 @@ void openqcd_to_soa(const Geo& g, const double* ud, const int* ipt, Links<T> U, 
 template <class T>
 void soa_to_openqcd(const Geo& g, Links<T> U, const int* ipt, double* ud, int mu0, int mu1,
                     cudaStream_t st);
-// Copy nlinks*9 complex entries between fields of possibly different precision.
-template <class D, class S>
-void convert(typename V2<D>::t* dst, const typename V2<S>::t* src, size_t n, cudaStream_t st);
 
 // ---- synthetic fields (gen_dev.cu) -----------------------------------------
 // Writes the synthetic link field of the given seed/eps straight into SoA.

@@ -20,15 +20,14 @@ __global__ void k_aos_to_soa(Geo g, const double2* __restrict__ aos, Links<T> U,
     int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
     int mu = mu0 + q;
     const double2* src = aos + 9 * ((size_t)4 * s + mu);
-    typename V2<T>::t* dst = U.p[mu];
+    M3<T> m;
 #pragma unroll
     for (int c = 0; c < 9; c++) {
       double2 v = src[c];
-      typename V2<T>::t o;
-      o.x = (T)v.x;
-      o.y = (T)v.y;
-      dst[(size_t)c * g.vol + s] = o;
+      m.e[c].x = (T)v.x;
+      m.e[c].y = (T)v.y;
     }
+    st(U.p[mu], g.vol, s, m);
   }
 }
 
@@ -40,12 +39,10 @@ __global__ void k_soa_to_aos(Geo g, Links<T> U, double2* __restrict__ aos, int m
     int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
     int mu = mu0 + q;
     double2* dst = aos + 9 * ((size_t)4 * s + mu);
-    const typename V2<T>::t* src = U.p[mu];
+    M3<T> m;
+    ld(m, U.p[mu], g.vol, s);
 #pragma unroll
-    for (int c = 0; c < 9; c++) {
-      typename V2<T>::t v = src[(size_t)c * g.vol + s];
-      dst[c] = make_double2((double)v.x, (double)v.y);
-    }
+    for (int c = 0; c < 9; c++) dst[c] = make_double2((double)m.e[c].x, (double)m.e[c].y);
   }
 }
 
@@ -69,14 +66,14 @@ __global__ void k_openqcd_to_soa(Geo g, const double2* __restrict__ ud, const in
     int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
     int mu = mu0 + q;
     const double2* src = ud + 9 * openqcd_ofs(g, ipt, s, mu);
+    M3<T> m;
 #pragma unroll
     for (int c = 0; c < 9; c++) {
       double2 v = src[c];
-      typename V2<T>::t o;
-      o.x = (T)v.x;
-      o.y = (T)v.y;
-      U.p[mu][(size_t)c * g.vol + s] = o;
+      m.e[c].x = (T)v.x;
+      m.e[c].y = (T)v.y;
     }
+    st(U.p[mu], g.vol, s, m);
   }
 }
 
@@ -89,23 +86,10 @@ __global__ void k_soa_to_openqcd(Geo g, Links<T> U, const int* __restrict__ ipt,
     int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
     int mu = mu0 + q;
     double2* dst = ud + 9 * openqcd_ofs(g, ipt, s, mu);
+    M3<T> m;
+    ld(m, U.p[mu], g.vol, s);
 #pragma unroll
-    for (int c = 0; c < 9; c++) {
-      typename V2<T>::t v = U.p[mu][(size_t)c * g.vol + s];
-      dst[c] = make_double2((double)v.x, (double)v.y);
-    }
-  }
-}
-
-template <class D, class S>
-__global__ void k_convert(typename V2<D>::t* dst, const typename V2<S>::t* src, size_t n) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    typename V2<S>::t v = src[i];
-    typename V2<D>::t o;
-    o.x = (D)v.x;
-    o.y = (D)v.y;
-    dst[i] = o;
+    for (int c = 0; c < 9; c++) dst[c] = make_double2((double)m.e[c].x, (double)m.e[c].y);
   }
 }
 
@@ -146,12 +130,6 @@ void soa_to_openqcd(const Geo& g, Links<T> U, const int* ipt, double* ud, int mu
       g, U, ipt, reinterpret_cast<double2*>(ud), mu0, nmu);
   WLG_LAUNCH_CHECK("soa_to_openqcd");
 }
-template <class D, class S>
-void convert(typename V2<D>::t* dst, const typename V2<S>::t* src, size_t n, cudaStream_t st) {
-  k_convert<D, S><<<grid_n((long long)n), 256, 0, st>>>(dst, src, n);
-  WLG_LAUNCH_CHECK("convert");
-}
-
 #define WLG_INST_L(T)                                                                       \
   template void aos_to_soa<T>(const Geo&, const double*, Links<T>, int, int, cudaStream_t); \
   template void soa_to_aos<T>(const Geo&, Links<T>, double*, int, int, cudaStream_t);       \
@@ -161,9 +139,5 @@ void convert(typename V2<D>::t* dst, const typename V2<S>::t* src, size_t n, cud
                                   cudaStream_t);
 WLG_INST_L(double)
 WLG_INST_L(float)
-template void convert<double, float>(double2*, const float2*, size_t, cudaStream_t);
-template void convert<float, double>(float2*, const double2*, size_t, cudaStream_t);
-template void convert<double, double>(double2*, const double2*, size_t, cudaStream_t);
-template void convert<float, float>(float2*, const float2*, size_t, cudaStream_t);
 
 }  // namespace wlg

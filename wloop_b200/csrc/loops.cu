@@ -33,10 +33,11 @@ __global__ void __launch_bounds__(128) k_line_step(Geo g, int msl, int R,
     coords(g, s, x);
     int y = shift(g, s, x[k + 1], k + 1, (R - 1) % g.n[k + 1]);
     M3<T> a, b, c;
-    ld(a, src + (size_t)q * 9 * g.vol, g.vol, s);
-    ld(b, level + (size_t)q * 9 * g.vol, g.vol, y);
+    const size_t off = (size_t)q * link_elems<T>(g.vol);
+    ld(a, src + off, g.vol, s);
+    ld(b, level + off, g.vol, y);
     mul(c, a, b);
-    st(dst + (size_t)q * 9 * g.vol, g.vol, s, c);
+    st(dst + off, g.vol, s, c);
   }
 }
 
@@ -118,7 +119,7 @@ __global__ void __launch_bounds__(128) k_contract(Geo g, const typename V2<T>::t
   const int per = (ncol + nCB - 1) / nCB;
   const int c_begin = cb * per;
   const int c_end = min(ncol, c_begin + per);
-  const size_t fstride = (size_t)9 * vol;
+  const size_t fstride = link_elems<T>(vol);
 
   // all lanes of a warp iterate together so shuffles stay converged
   for (int cbase = c_begin; cbase < c_end; cbase += blockDim.x) {
@@ -184,7 +185,119 @@ __global__ void __launch_bounds__(128) k_contract(Geo g, const typename V2<T>::t
     }
   }
   __syncthreads();
-  double* out = partial + (size_t)blockIdx.x * rowlen;
+  // partial layout [x0][grp][cb] (read back by k_contract_reduce)
+  double* out = partial + ((size_t)(x0 * ngrp + grp) * nCB + cb) * rowlen;
+  for (int i = threadIdx.x; i < rowlen; i += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < nwarps; w++) s += acc[(size_t)w * rowlen + i];
+    out[i] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// contraction kernel, second form: same work split as k_contract, with
+//  * C updated in place (6 temporaries per product instead of a full matrix),
+//  * the next T-step's temporal links loaded right after they are consumed,
+//    so their latency overlaps the traces and the reduction,
+//  * the top levels taken SB at a time in a rolled loop with a K=G*SB shuffle
+//    reduction (small register footprint, compact code),
+//  * __launch_bounds__ minimum-blocks hint so three or more blocks fit an SM.
+// ---------------------------------------------------------------------------
+template <class T, int G, int SB, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_contract2(Geo g,
+                                                         const typename V2<T>::t* __restrict__ u0,
+                                                         const typename V2<T>::t* __restrict__ lines,
+                                                         int msl, int mwlt, int R, int ngrp,
+                                                         int nCB, double* __restrict__ partial) {
+  extern __shared__ double acc[];  // [nwarps][mwlt][G][msl]
+  constexpr int K = G * SB;
+  constexpr int KP = Pow2<K>::v;
+  static_assert(K <= 32, "G*SB must not exceed 32");
+
+  const int N0 = g.n[0], vs = g.vs, vol = g.vol;
+  int b = blockIdx.x;
+  const int x0 = b % N0;
+  b /= N0;
+  const int grp = b % ngrp;
+  const int cb = b / ngrp;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int rowlen = mwlt * G * msl;
+  double* wacc = acc + (size_t)warp * rowlen;
+  for (int i = lane; i < rowlen; i += 32) wacc[i] = 0.0;
+  __syncwarp();
+
+  const int s1_0 = grp * G;
+  const int ncol = 3 * vs;
+  const int per = (ncol + nCB - 1) / nCB;
+  const int c_begin = cb * per;
+  const int c_end = min(ncol, c_begin + per);
+  const size_t fstride = link_elems<T>(vol);
+  const int idx = lane >> (5 - Log2<KP>::v);
+  const bool writer = (lane & ((32 / KP) - 1)) == 0 && idx < K;
+  const int wg = idx / SB, wj = idx % SB;
+
+  for (int cbase = c_begin; cbase < c_end; cbase += blockDim.x) {
+    const int col = cbase + threadIdx.x;
+    const bool active = col < c_end;
+    const int cc = active ? col : c_begin;
+    const int k = cc / vs, xs = cc - k * vs;
+    int xsR;
+    {
+      // xs + R k inside the time slice (selects, no local-memory array)
+      const int x1 = xs / g.st[1], r = xs - x1 * g.st[1];
+      const int x2 = r / g.st[2], x3 = r - x2 * g.st[2];
+      const int xk = (k == 0) ? x1 : ((k == 1) ? x2 : x3);
+      const int nk = g.n[k + 1];
+      int y = xk + (R % nk);
+      if (y >= nk) y -= nk;
+      xsR = xs + (y - xk) * g.st[k + 1];
+    }
+    const typename V2<T>::t* lk = lines + (size_t)k * fstride;  // level s stride 3*fstride
+    M3<T> C[G];
+#pragma unroll
+    for (int gi = 0; gi < G; gi++) {
+      int s1 = min(s1_0 + gi, msl - 1);
+      ld(C[gi], lk + (size_t)s1 * 3 * fstride, vol, x0 * vs + xs);
+    }
+    M3<T> ua, ub;
+    ld(ua, u0, vol, x0 * vs + xs);
+    ld(ub, u0, vol, x0 * vs + xsR);
+    int t0 = x0;
+    for (int tt = 1; tt <= mwlt; tt++) {
+#pragma unroll
+      for (int gi = 0; gi < G; gi++) lmul_dag_inplace(C[gi], ua);
+#pragma unroll
+      for (int gi = 0; gi < G; gi++) rmul_inplace(C[gi], ub);
+      t0 = (t0 + 1 == N0) ? 0 : t0 + 1;  // x0+T mod N0: top slice, next bottom link slice
+      if (tt < mwlt) {
+        ld(ua, u0, vol, t0 * vs + xs);
+        ld(ub, u0, vol, t0 * vs + xsR);
+      }
+      const int stop = t0 * vs + xs;
+      double* arow = wacc + (size_t)(tt - 1) * G * msl;
+#pragma unroll 1
+      for (int sb = 0; sb < msl; sb += SB) {
+        double v[KP];
+#pragma unroll
+        for (int i = 0; i < KP; i++) v[i] = 0.0;
+#pragma unroll
+        for (int j = 0; j < SB; j++) {
+          const int s2 = sb + j;
+          if (s2 < msl) {
+            M3<T> l;
+            ld(l, lk + (size_t)s2 * 3 * fstride, vol, stop);
+#pragma unroll
+            for (int gi = 0; gi < G; gi++)
+              v[gi * SB + j] = active ? (double)retr_dag(l, C[gi]) : 0.0;
+          }
+        }
+        double sum = wt_reduce<KP>(v, lane);
+        if (writer && sb + wj < msl) arow[wg * msl + sb + wj] += sum;
+      }
+    }
+  }
+  __syncthreads();
+  double* out = partial + ((size_t)(x0 * ngrp + grp) * nCB + cb) * rowlen;
   for (int i = threadIdx.x; i < rowlen; i += blockDim.x) {
     double s = 0.0;
     for (int w = 0; w < nwarps; w++) s += acc[(size_t)w * rowlen + i];
@@ -197,18 +310,20 @@ ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hin
   ContractPlan p;
   int G = G_hint;
   if (G <= 0) {
-    if (fp64) {
-      G = (msl % 3 == 0 || msl > 4) ? 3 : (msl >= 2 ? 2 : 1);
-      if (msl == 4) G = 2;
-    } else {
-      G = msl <= 6 ? msl : (msl % 4 == 0 ? 4 : 4);
-    }
+    // two level groups for msl >= 4 (C of G levels stays in registers), one below
+    G = (msl <= 3) ? msl : (msl + 1) / 2;
+    if (fp64 && G > 3) G = 3;
   }
   if (G > msl) G = msl;
   if (G < 1) G = 1;
+  if (G == 5) G = 6;
   p.G = G;
+  p.SB = (msl >= 2 && G <= 4 && !(fp64 && G >= 3)) ? 2 : 1;
+  // third form (staged top lines) unless G = 6, which only the second form has
+  p.variant = (G <= 4) ? 3 : 2;
   p.ngrp = (msl + G - 1) / G;
-  p.block = block_hint > 0 ? block_hint : 128;
+  // FP64 stages twice the bytes per thread: 64-thread blocks keep 3 blocks per SM
+  p.block = block_hint > 0 ? block_hint : ((fp64 && p.variant == 3) ? 64 : 128);
   int ncol = 3 * g.vs;
   int nCB = nCB_hint;
   if (nCB <= 0) {
@@ -225,6 +340,29 @@ ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hin
   return p;
 }
 
+template <class T, int G, int SB>
+static void launch_contract2(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
+                             const typename V2<T>::t* lines, int msl, int mwlt, int R,
+                             double* partial, cudaStream_t st) {
+  constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
+  auto kern = k_contract2<T, G, SB, MINB>;
+  if (p.smem > 48 * 1024)
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+  int grid = g.n[0] * p.ngrp * p.nCB;
+  kern<<<grid, p.block, p.smem, st>>>(g, u0, lines, msl, mwlt, R, p.ngrp, p.nCB, partial);
+  WLG_LAUNCH_CHECK("contract");
+}
+
+template <class T, int G>
+static void launch_contract2_sb(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
+                                const typename V2<T>::t* lines, int msl, int mwlt, int R,
+                                double* partial, cudaStream_t st) {
+  if (p.SB == 2)
+    launch_contract2<T, G, 2>(g, p, u0, lines, msl, mwlt, R, partial, st);
+  else
+    launch_contract2<T, G, 1>(g, p, u0, lines, msl, mwlt, R, partial, st);
+}
+
 template <class T, int G>
 static void launch_contract_G(const Geo& g, const ContractPlan& p,
                               const typename V2<T>::t* u0, const typename V2<T>::t* lines,
@@ -238,17 +376,219 @@ static void launch_contract_G(const Geo& g, const ContractPlan& p,
   WLG_LAUNCH_CHECK("contract");
 }
 
+// ---------------------------------------------------------------------------
+// contraction kernel, third form: the second form plus asynchronous staging
+// of the top-level lines.  At the start of every T-step each thread issues
+// cp.async copies of its msl top lines (slice x0+T) into its own
+// shared-memory slots, then runs the 2G matrix products of the recursion
+// while the copies are in flight, and reads the lines back from shared
+// memory for the traces.  Slots are laid out [level][16-byte chunk][thread]
+// so the copies and the reads of a warp are bank-conflict free.
+// ---------------------------------------------------------------------------
+template <class T> struct Chunks;
+template <> struct Chunks<double> { enum { N = 9 }; };  // 9 x double2 per link
+template <> struct Chunks<float> { enum { N = 5 }; };   // 5 x float4 per link (tiled pairs)
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// 16-byte chunk q of link s in a tiled direction array (common.cuh layout)
+template <class T> __device__ __forceinline__ const char* chunk_ptr(const typename V2<T>::t* base, int s, int q);
+template <> __device__ __forceinline__ const char* chunk_ptr<double>(const double2* base, int s, int q) {
+  return reinterpret_cast<const char*>(base + (size_t)(s >> 5) * 288 + q * 32 + (s & 31));
+}
+template <> __device__ __forceinline__ const char* chunk_ptr<float>(const float2* base, int s, int q) {
+  return reinterpret_cast<const char*>(reinterpret_cast<const float4*>(base) + (size_t)(s >> 5) * 160 +
+                                       q * 32 + (s & 31));
+}
+template <class T> __device__ __forceinline__ void ld_stage(M3<T>& m, const char* slot, int stride);
+template <> __device__ __forceinline__ void ld_stage<double>(M3<double>& m, const char* slot, int stride) {
+#pragma unroll
+  for (int q = 0; q < 9; q++) m.e[q] = *reinterpret_cast<const double2*>(slot + q * stride);
+}
+template <> __device__ __forceinline__ void ld_stage<float>(M3<float>& m, const char* slot, int stride) {
+#pragma unroll
+  for (int q = 0; q < 5; q++) {
+    float4 v = *reinterpret_cast<const float4*>(slot + q * stride);
+    m.e[2 * q] = make_float2(v.x, v.y);
+    if (q < 4) m.e[2 * q + 1] = make_float2(v.z, v.w);
+  }
+}
+
+template <class T, int G, int SB, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_contract3(Geo g,
+                                                         const typename V2<T>::t* __restrict__ u0,
+                                                         const typename V2<T>::t* __restrict__ lines,
+                                                         int msl, int mwlt, int R, int ngrp,
+                                                         int nCB, double* __restrict__ partial) {
+  extern __shared__ double acc[];  // [nwarps][mwlt][G][msl] doubles, then the line stage
+  constexpr int K = G * SB;
+  constexpr int KP = Pow2<K>::v;
+  constexpr int NQ = Chunks<T>::N;
+  static_assert(K <= 32, "G*SB must not exceed 32");
+
+  const int N0 = g.n[0], vs = g.vs, vol = g.vol;
+  int b = blockIdx.x;
+  const int x0 = b % N0;
+  b /= N0;
+  const int grp = b % ngrp;
+  const int cb = b / ngrp;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int rowlen = mwlt * G * msl;
+  double* wacc = acc + (size_t)warp * rowlen;
+  // line stage: [msl][NQ][blockDim] 16-byte chunks; this thread's slot of chunk (s2,q)
+  char* stage = reinterpret_cast<char*>(acc + (size_t)nwarps * rowlen);
+  const int qstride = blockDim.x * 16;
+  char* myslot = stage + threadIdx.x * 16;
+  for (int i = lane; i < rowlen; i += 32) wacc[i] = 0.0;
+  __syncwarp();
+
+  const int s1_0 = grp * G;
+  const int ncol = 3 * vs;
+  const int per = (ncol + nCB - 1) / nCB;
+  const int c_begin = cb * per;
+  const int c_end = min(ncol, c_begin + per);
+  const size_t fstride = link_elems<T>(vol);
+  const int idx = lane >> (5 - Log2<KP>::v);
+  const bool writer = (lane & ((32 / KP) - 1)) == 0 && idx < K;
+  const int wg = idx / SB, wj = idx % SB;
+
+  for (int cbase = c_begin; cbase < c_end; cbase += blockDim.x) {
+    const int col = cbase + threadIdx.x;
+    const bool active = col < c_end;
+    const int cc = active ? col : c_begin;
+    const int k = cc / vs, xs = cc - k * vs;
+    int xsR;
+    {
+      const int x1 = xs / g.st[1], r = xs - x1 * g.st[1];
+      const int x2 = r / g.st[2], x3 = r - x2 * g.st[2];
+      const int xk = (k == 0) ? x1 : ((k == 1) ? x2 : x3);
+      const int nk = g.n[k + 1];
+      int y = xk + (R % nk);
+      if (y >= nk) y -= nk;
+      xsR = xs + (y - xk) * g.st[k + 1];
+    }
+    const typename V2<T>::t* lk = lines + (size_t)k * fstride;
+    const size_t lvl = 3 * fstride;
+    M3<T> C[G];
+#pragma unroll
+    for (int gi = 0; gi < G; gi++) {
+      int s1 = min(s1_0 + gi, msl - 1);
+      ld(C[gi], lk + (size_t)s1 * lvl, vol, x0 * vs + xs);
+    }
+    M3<T> ua, ub;
+    ld(ua, u0, vol, x0 * vs + xs);
+    ld(ub, u0, vol, x0 * vs + xsR);
+    int t0 = x0;
+    for (int tt = 1; tt <= mwlt; tt++) {
+      const int t1 = (t0 + 1 == N0) ? 0 : t0 + 1;  // x0+T mod N0: the top slice
+      const int stop = t1 * vs + xs;
+      // stage the msl top lines of this step (own slots: no block barrier needed)
+      for (int s2 = 0; s2 < msl; s2++) {
+        const typename V2<T>::t* src = lk + (size_t)s2 * lvl;
+#pragma unroll
+        for (int q = 0; q < NQ; q++)
+          cp_async16(myslot + (s2 * NQ + q) * qstride, chunk_ptr<T>(src, stop, q));
+      }
+      cp_async_commit();
+#pragma unroll
+      for (int gi = 0; gi < G; gi++) lmul_dag_inplace(C[gi], ua);
+#pragma unroll
+      for (int gi = 0; gi < G; gi++) rmul_inplace(C[gi], ub);
+      t0 = t1;
+      if (tt < mwlt) {
+        ld(ua, u0, vol, t0 * vs + xs);
+        ld(ub, u0, vol, t0 * vs + xsR);
+      }
+      cp_async_wait_all();
+      double* arow = wacc + (size_t)(tt - 1) * G * msl;
+#pragma unroll 1
+      for (int sb = 0; sb < msl; sb += SB) {
+        double v[KP];
+#pragma unroll
+        for (int i = 0; i < KP; i++) v[i] = 0.0;
+#pragma unroll
+        for (int j = 0; j < SB; j++) {
+          const int s2 = sb + j;
+          if (s2 < msl) {
+            M3<T> l;
+            ld_stage<T>(l, myslot + s2 * NQ * qstride, qstride);
+#pragma unroll
+            for (int gi = 0; gi < G; gi++)
+              v[gi * SB + j] = active ? (double)retr_dag(l, C[gi]) : 0.0;
+          }
+        }
+        double sum = wt_reduce<KP>(v, lane);
+        if (writer && sb + wj < msl) arow[wg * msl + sb + wj] += sum;
+      }
+    }
+  }
+  __syncthreads();
+  double* out = partial + ((size_t)(x0 * ngrp + grp) * nCB + cb) * rowlen;
+  for (int i = threadIdx.x; i < rowlen; i += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < nwarps; w++) s += acc[(size_t)w * rowlen + i];
+    out[i] = s;
+  }
+}
+
+template <class T, int G, int SB>
+static void launch_contract3(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
+                             const typename V2<T>::t* lines, int msl, int mwlt, int R,
+                             double* partial, cudaStream_t st) {
+  constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
+  auto kern = k_contract3<T, G, SB, MINB>;
+  size_t smem = p.smem + (size_t)msl * Chunks<T>::N * p.block * 16;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int grid = g.n[0] * p.ngrp * p.nCB;
+  kern<<<grid, p.block, smem, st>>>(g, u0, lines, msl, mwlt, R, p.ngrp, p.nCB, partial);
+  WLG_LAUNCH_CHECK("contract");
+}
+
+template <class T, int G>
+static void launch_contract3_sb(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
+                                const typename V2<T>::t* lines, int msl, int mwlt, int R,
+                                double* partial, cudaStream_t st) {
+  if (p.SB == 2)
+    launch_contract3<T, G, 2>(g, p, u0, lines, msl, mwlt, R, partial, st);
+  else
+    launch_contract3<T, G, 1>(g, p, u0, lines, msl, mwlt, R, partial, st);
+}
+
 template <class T>
 void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
               const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
               cudaStream_t st) {
+  if (p.variant == 1) {
+    switch (p.G) {
+      case 1: launch_contract_G<T, 1>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      case 2: launch_contract_G<T, 2>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      case 3: launch_contract_G<T, 3>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      case 4: launch_contract_G<T, 4>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      case 6: launch_contract_G<T, 6>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      default: set_error("contract: unsupported G=%d", p.G); return;
+    }
+  }
+  if (p.variant == 3) {
+    switch (p.G) {
+      case 1: launch_contract3_sb<T, 1>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      case 2: launch_contract3_sb<T, 2>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      case 3: launch_contract3_sb<T, 3>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      case 4: launch_contract3_sb<T, 4>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      default: break;  // G=6 falls through to the second form
+    }
+  }
   switch (p.G) {
-    case 1: launch_contract_G<T, 1>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
-    case 2: launch_contract_G<T, 2>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
-    case 3: launch_contract_G<T, 3>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
-    case 4: launch_contract_G<T, 4>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
-    case 5: launch_contract_G<T, 5>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
-    case 6: launch_contract_G<T, 6>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 1: launch_contract2_sb<T, 1>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 2: launch_contract2_sb<T, 2>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 3: launch_contract2_sb<T, 3>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 4: launch_contract2_sb<T, 4>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 6: launch_contract2<T, 6, 1>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
     default: set_error("contract: unsupported G=%d", p.G);
   }
 }

@@ -38,7 +38,7 @@ static inline int grid_for(long long n, int block) {
 template <class T>
 __device__ __forceinline__ typename V2<T>::t* fld(typename V2<T>::t* base, int vol, int slot, int mu,
                                                   int ndir) {
-  return base + (size_t)(slot * ndir + mu) * 9 * vol;
+  return base + (size_t)(slot * ndir + mu) * link_elems<T>(vol);
 }
 
 // v = a*u + b*s (FP64), then optional projection; this is _su3_lcomb +
