@@ -128,6 +128,13 @@ int wlg_staple_sum(const int n[4], const double* u1, const double* u2, int mu, i
 /* In-place projection of nmat packed su3_dble matrices
  * (approx_project_to_su3_dble, projection.c:120-154). */
 int wlg_project(double* mats, int nmat, int iter);
+/* v[i] += staple of the link triple (u1[i],u2[i],u3[i]) for nmat packed
+ * su3_dble: dn = 0 up staple u1 u2 u3^dag, dn = 1 down staple u1^dag u2 u3;
+ * save = 1 general 3x3 form (add_*_staple_lnks_save, lnkstaple.c:385-410),
+ * save = 0 SU(3) form with the third column rebuilt (add_*_staple_lnks,
+ * lnkstaple.c:296-315). */
+int wlg_staples(int nmat, const double* u1, const double* u2, const double* u3, double* v, int dn,
+                int save);
 
 /* ---- kernel timing (CUDA events on the context's stream) ------------------ */
 int wlg_set_profiling(wlg_ctx* ctx, int on);

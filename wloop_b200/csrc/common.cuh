@@ -254,61 +254,6 @@ template <class T> __device__ __forceinline__ void rmul_inplace(M3<T>& c, const 
   }
 }
 
-// FP32 forms on the packed FP32x2 FMA of sm_100 (__ffma2_rn): a complex
-// multiply-accumulate x*y is (x.re,x.re)*(y.re,y.im) + (x.im,x.im)*(-y.im,y.re),
-// i.e. two packed FMAs instead of four scalar ones.
-__device__ __forceinline__ float2 pk(float a, float b) { return make_float2(a, b); }
-
-template <> __device__ __forceinline__ void lmul_dag_inplace<float>(M3<float>& c, const M3<float>& a) {
-  // out[i][j] = sum_k conj(a[k][i]) c[k][j];
-  // conj(a) x = (a.x,a.x)*(x.x,x.y) + (a.y,-a.y)*(x.y,x.x)
-  float2 ax[9], ay[9];
-#pragma unroll
-  for (int t = 0; t < 9; t++) {
-    ax[t] = pk(a.e[t].x, a.e[t].x);
-    ay[t] = pk(a.e[t].y, -a.e[t].y);
-  }
-#pragma unroll
-  for (int j = 0; j < 3; j++) {
-    const float2 x0 = c.e[j], x1 = c.e[3 + j], x2 = c.e[6 + j];
-    const float2 s0 = pk(x0.y, x0.x), s1 = pk(x1.y, x1.x), s2 = pk(x2.y, x2.x);
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-      float2 o = __fmul2_rn(ax[i], x0);
-      o = __ffma2_rn(ay[i], s0, o);
-      o = __ffma2_rn(ax[3 + i], x1, o);
-      o = __ffma2_rn(ay[3 + i], s1, o);
-      o = __ffma2_rn(ax[6 + i], x2, o);
-      o = __ffma2_rn(ay[6 + i], s2, o);
-      c.e[3 * i + j] = o;
-    }
-  }
-}
-
-template <> __device__ __forceinline__ void rmul_inplace<float>(M3<float>& c, const M3<float>& b) {
-  // out[i][j] = sum_k c[i][k] b[k][j];  x b = (x.x,x.x)*b + (x.y,x.y)*(-b.y,b.x)
-  float2 bp[9];
-#pragma unroll
-  for (int t = 0; t < 9; t++) bp[t] = pk(-b.e[t].y, b.e[t].x);
-#pragma unroll
-  for (int i = 0; i < 3; i++) {
-    const float2 x0 = c.e[3 * i], x1 = c.e[3 * i + 1], x2 = c.e[3 * i + 2];
-    const float2 r0 = pk(x0.x, x0.x), i0 = pk(x0.y, x0.y);
-    const float2 r1 = pk(x1.x, x1.x), i1 = pk(x1.y, x1.y);
-    const float2 r2 = pk(x2.x, x2.x), i2 = pk(x2.y, x2.y);
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      float2 o = __fmul2_rn(r0, b.e[j]);
-      o = __ffma2_rn(i0, bp[j], o);
-      o = __ffma2_rn(r1, b.e[3 + j], o);
-      o = __ffma2_rn(i1, bp[3 + j], o);
-      o = __ffma2_rn(r2, b.e[6 + j], o);
-      o = __ffma2_rn(i2, bp[6 + j], o);
-      c.e[3 * i + j] = o;
-    }
-  }
-}
-
 template <class T> __device__ __forceinline__ void acc(M3<T>& c, const M3<T>& a) {
 #pragma unroll
   for (int k = 0; k < 9; k++) {
@@ -317,24 +262,17 @@ template <class T> __device__ __forceinline__ void acc(M3<T>& c, const M3<T>& a)
   }
 }
 
-// Re tr(a^dag b) = sum_ij Re(conj(a_ij) b_ij)  (openQCD _vector_prod_re over rows)
+// Re tr(a^dag b) = sum_ij Re(conj(a_ij) b_ij)  (openQCD _vector_prod_re over rows),
+// accumulated as two independent partial sums (real and imaginary parts).
 template <class T> __device__ __forceinline__ T retr_dag(const M3<T>& a, const M3<T>& b) {
   T s = a.e[0].x * b.e[0].x;
-  s = fma(a.e[0].y, b.e[0].y, s);
+  T t = a.e[0].y * b.e[0].y;
 #pragma unroll
   for (int k = 1; k < 9; k++) {
     s = fma(a.e[k].x, b.e[k].x, s);
-    s = fma(a.e[k].y, b.e[k].y, s);
+    t = fma(a.e[k].y, b.e[k].y, t);
   }
-  return s;
-}
-
-// FP32: (sum a.x b.x, sum a.y b.y) in one packed accumulator
-template <> __device__ __forceinline__ float retr_dag<float>(const M3<float>& a, const M3<float>& b) {
-  float2 s = __fmul2_rn(a.e[0], b.e[0]);
-#pragma unroll
-  for (int k = 1; k < 9; k++) s = __ffma2_rn(a.e[k], b.e[k], s);
-  return s.x + s.y;
+  return s + t;
 }
 
 template <class D, class S> __device__ __forceinline__ void cvt(M3<D>& d, const M3<S>& s) {

@@ -736,6 +736,29 @@ int wlg_project(double* mats, int nmat, int iter) {
   return finish("project");
 }
 
+int wlg_staples(int nmat, const double* u1, const double* u2, const double* u3, double* v, int dn,
+                int save) {
+  set_error("%s", "");
+  if (nmat <= 0) return 0;
+  if (wlg_device_count() <= 0) {
+    set_error("no CUDA device available (the wloop_b200 path has no CPU fallback)");
+    return -1;
+  }
+  size_t bytes = sizeof(double) * 18 * (size_t)nmat;
+  DevBuf b;
+  if (ensure(b, 4 * bytes)) return -1;
+  char* p = (char*)b.p;
+  WLG_CUDA(cudaMemcpy(p, u1, bytes, cudaMemcpyHostToDevice));
+  WLG_CUDA(cudaMemcpy(p + bytes, u2, bytes, cudaMemcpyHostToDevice));
+  WLG_CUDA(cudaMemcpy(p + 2 * bytes, u3, bytes, cudaMemcpyHostToDevice));
+  WLG_CUDA(cudaMemcpy(p + 3 * bytes, v, bytes, cudaMemcpyHostToDevice));
+  staples_lnks(nmat, (const double*)p, (const double*)(p + bytes), (const double*)(p + 2 * bytes),
+               (double*)(p + 3 * bytes), dn, save, 0);
+  WLG_CUDA(cudaMemcpy(v, p + 3 * bytes, bytes, cudaMemcpyDeviceToHost));
+  release(b);
+  return finish("staples");
+}
+
 int wlg_set_profiling(wlg_ctx* c, int on) {
   CTX_BEGIN(c);
   harvest(c);

@@ -44,6 +44,10 @@ void hyp3d_level2(const Geo& g, Links<T> U, const typename V2<T>::t* dl, double 
 template <class T>
 void staple_sum(const Geo& g, Links<T> u1, Links<T> u2, int mu, int nu, Links<T> vb,
                 cudaStream_t st);
+// v[i] += staple(u1[i],u2[i],u3[i]) for n packed FP64 matrices (dn: down
+// staple; save: general form, else SU(3) third-column form).
+void staples_lnks(int n, const double* u1, const double* u2, const double* u3, double* v, int dn,
+                  int save, cudaStream_t st);
 // In-place projection of n packed FP64 matrices (18 doubles each).
 void project_batch(double* m, int n, int iter, cudaStream_t st);
 // Plaquette sum (lnkplaq.c:48-128) into *out (device double); partial holds

@@ -331,6 +331,61 @@ __global__ void k_sum_partials(const double* partial, int n, double* out) {
 }
 
 // ---------------------------------------------------------------------------
+// Single staples on explicit link triples (add_*_staple_lnks[_save],
+// lnkstaple.c:145-410).  save = 1: general 3x3 form v += u1 u2 u3^dag (up)
+// or u1^dag u2 u3 (down).  save = 0: the SU(3) form of up_staple/dn_staple
+// (:145-256): only the first two columns of the product are formed and the
+// third is added as conj(col1 x col2) (add_to_v, :108-142).
+// Matrices are packed su3_dble (18 doubles), FP64.
+// ---------------------------------------------------------------------------
+__global__ void k_staples_lnks(int n, const double2* u1, const double2* u2, const double2* u3,
+                               double2* v, int dn, int save) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    M3<double> a, b, c, t, r;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      a.e[k] = u1[9 * (size_t)i + k];
+      b.e[k] = u2[9 * (size_t)i + k];
+      c.e[k] = u3[9 * (size_t)i + k];
+    }
+    if (dn) {
+      mul(t, b, c);
+      mul_da(r, a, t);
+    } else {
+      mul_ad(t, b, c);
+      mul(r, a, t);
+    }
+    if (!save) {
+      // third column from the first two: c_i3 = conj(c1 x c2)_i
+#pragma unroll
+      for (int row = 0; row < 3; row++) {
+        int p = (row + 1) % 3, q = (row + 2) % 3;
+        double2 x1 = r.e[3 * p], y2 = r.e[3 * q + 1], x2 = r.e[3 * q], y1 = r.e[3 * p + 1];
+        double re = (x1.x * y2.x - x1.y * y2.y) - (x2.x * y1.x - x2.y * y1.y);
+        double im = (x1.x * y2.y + x1.y * y2.x) - (x2.x * y1.y + x2.y * y1.x);
+        r.e[3 * row + 2] = make_double2(re, -im);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      double2 o = v[9 * (size_t)i + k];
+      o.x += r.e[k].x;
+      o.y += r.e[k].y;
+      v[9 * (size_t)i + k] = o;
+    }
+  }
+}
+
+void staples_lnks(int n, const double* u1, const double* u2, const double* u3, double* v, int dn,
+                  int save, cudaStream_t st) {
+  if (n <= 0) return;
+  k_staples_lnks<<<grid_for(n, 128), 128, 0, st>>>(
+      n, reinterpret_cast<const double2*>(u1), reinterpret_cast<const double2*>(u2),
+      reinterpret_cast<const double2*>(u3), reinterpret_cast<double2*>(v), dn, save);
+  WLG_LAUNCH_CHECK("staples_lnks");
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 template <class T>
