@@ -136,6 +136,24 @@ int wlg_project(double* mats, int nmat, int iter);
 int wlg_staples(int nmat, const double* u1, const double* u2, const double* u3, double* v, int dn,
                 int save);
 
+/* ---- plaquette sum without device allocation -------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory at this point (memory owned by another allocator or a preallocated
+ * arena; a latency-critical path where cudaMalloc/cudaFree would synchronise
+ * the device): the same sum as wlg_plaq_sum, from a su3_dble field the caller
+ * already holds in device memory.  links: 4*V links in AoS lexicographic order
+ * (device or managed memory); out: one double in device memory, written when
+ * the work on `stream` (a cudaStream_t, 0 = default stream) completes.
+ * Its only scratch is a fixed array inside the library (128 KiB per GPU that
+ * loads the library, held until exit), so lattices above
+ * WLG_NOALLOC_MAX_SITES sites are rejected.  The first call on a device looks
+ * up that array's device address (cudaGetSymbolAddress) and should come
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race and must not be issued.  It calls no cudaMalloc, cudaFree
+ * or other allocating routine. */
+#define WLG_NOALLOC_MAX_SITES 33554432
+int wlg_plaq_sum_noalloc(const double* links, const int n[4], int bc, double* out, void* stream);
+
 /* ---- kernel timing (CUDA events on the context's stream) ------------------ */
 int wlg_set_profiling(wlg_ctx* ctx, int on);
 /* name: "hyp", "ape", "plaq", "lines", "contract", "reduce" */
