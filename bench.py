@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -54,6 +55,11 @@ def parse():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--lattice", default=None,
                     help="N0xN1xN2xN3 override for small profiling captures (not a bench line)")
+    ap.add_argument("--workload", default="c3", choices=["c3", "c4", "c5"],
+                    help="c3: headline single configuration; c4: 64-configuration batch in one "
+                         "graph launch; c5: serving loop with Poisson arrivals")
+    ap.add_argument("--requests", type=int, default=100, help="c5: number of requests")
+    ap.add_argument("--rate", type=float, default=20.0, help="c5: arrivals per second")
     return ap.parse_args()
 
 
@@ -340,6 +346,96 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_batch(args):
+    """c4: 48 x 16^3x32 + 16 x 24^3x48, HYP2 + 4 APE levels, r,t <= Ns/2, mixed
+    precision, all 64 configurations in one CUDA-graph launch per step."""
+    import numpy as np
+    import torch
+    from wloop_b200.api import Batch, launch_count
+    from wloop_b200.autotune import tune_batch
+    from wloop_b200.workloads import batch_workloads, flops_per_config
+    ws = batch_workloads()
+    prec = args.precision
+    b = Batch([(w.n, w.bc, w.parms) for w in ws], prec)
+    b.generate([w.seed for w in ws], [w.eps for w in ws])
+    shape = tune_batch(b)
+    b.snapshot()
+    for _ in range(args.warmup):
+        b.restore()
+        b.run()
+    ext = torch.cuda.ExternalStream(b.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    l0 = launch_count()
+    e0.record(ext)
+    for _ in range(args.steps):
+        b.restore()
+        b.run()
+    e1.record(ext)
+    e1.synchronize()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    _, kern = b.stats()
+    flops = sum(flops_per_config(w)["total"] for w in ws)
+    line = {"metric": "configs/s, 64-configuration batch (48 x 16^3x32 + 16 x 24^3x48)",
+            "value": len(ws) * 1000.0 / ms, "unit": "configs/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": "c4 batch, HYP2 + APE 0.5 nss 0 5 5 5, r,t <= Ns/2, one graph "
+                                   "launch per step", "precision": prec,
+                       "contract_shape_GSBblocknCB": list(shape),
+                       "device_bytes": b.device_bytes},
+            "kernels_per_graph": kern, "gpu_launches_device_side": kern * args.steps,
+            "host_launch_calls": launch_count() - l0,
+            "algorithmic_tflops": flops / (ms * 1e-3) / 1e12, "clocks": ck}
+    b.close()
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """c5: measurement requests with Poisson arrivals (rate --rate) over the
+    volumes {16^3x32, 24^3x48, 32^3x64, 48^3x96}, eps ~ U[0.15,0.35], bc
+    open/periodic 50/50, HYP2 + 4 APE levels, r,t <= Ns/2; p50/p99 latency and
+    throughput for the mixed and the FP64 forms."""
+    import random
+    from wloop_b200.api import Server, aux_uniform
+    from wloop_b200.workloads import serving_request
+    out = {"metric": "serving: p50/p99 latency (ms) and configs/s, Poisson arrivals",
+           "unit": "configs/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+           "requests": args.requests, "rate_per_s": args.rate, "forms": {}}
+    for prec, nreq in (("mixed", args.requests), ("fp64", max(10, args.requests // 3))):
+        reqs = [serving_request(i) for i in range(nreq)]
+        t = 0.0
+        arrivals = []
+        for i in range(nreq):  # exponential inter-arrival times from the seeded stream
+            u = aux_uniform(5000, i, 7)
+            t += -math.log(1.0 - u) / args.rate
+            arrivals.append(t)
+        with Server(max_inflight=3, max_batch=8, mem_fraction=0.85) as s:
+            t0 = time.perf_counter()
+            ids = []
+            for w, ta in zip(reqs, arrivals):
+                dt = ta - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                ids.append(s.submit(w.n, w.bc, w.parms, prec, seed=w.seed, eps=w.eps))
+            for i in ids:
+                s.wait(i)
+            st = s.stats()
+        mix = {}
+        for w in reqs:
+            key = "x".join(str(v) for v in (w.n[1], w.n[1], w.n[1], w.n[0]))
+            mix[key] = mix.get(key, 0) + 1
+        out["forms"][prec] = {"requests": nreq, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                              "configs_per_s": st["throughput"], "batches": st["batches"],
+                              "failed": st["failed"], "volume_mix": mix}
+    out["value"] = out["forms"]["mixed"]["configs_per_s"]
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -347,6 +443,12 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "c4":
+        run_batch(args)
+        return
+    if args.workload == "c5":
+        run_serve(args)
         return
     run_ours(args, rank, world, local)
 

@@ -136,6 +136,76 @@ int wlg_project(double* mats, int nmat, int iter);
 int wlg_staples(int nmat, const double* u1, const double* u2, const double* u3, double* v, int dn,
                 int save);
 
+/* ---- batches: many configurations measured in one CUDA-graph launch --------
+ * No counterpart in the reference (ms10 measures one configuration at a
+ * time, main/ms10.c:701-742).  A batch holds nconf configurations of
+ * possibly different lattices (dims[4*c..4*c+3], bcs[c], parms[c]) on one
+ * GPU; wlg_batch_run applies to every one of them what wlg_measure applies to
+ * one (HYP with alpha_action, the smearing levels, all Wilson loops) with each
+ * stage as one kernel over all configurations, the whole sequence captured
+ * into a CUDA graph on the first run and replayed afterwards. */
+typedef struct wlg_batch wlg_batch;
+int wlg_batch_create(int nconf, const int* dims, const int* bcs, const wlg_wloop_parms* parms,
+                     int precision, int device, wlg_batch** out);
+int wlg_batch_destroy(wlg_batch* b);
+int wlg_batch_size(wlg_batch* b);
+/* device bytes held by the batch's field arena */
+long long wlg_batch_bytes(wlg_batch* b);
+/* gauge field of configuration i from a host AoS su3_dble buffer */
+int wlg_batch_upload(wlg_batch* b, int i, const double* aos);
+/* synthetic fields for all configurations on the device */
+int wlg_batch_generate(wlg_batch* b, const uint64_t* seeds, const double* eps);
+int wlg_batch_snapshot(wlg_batch* b);
+int wlg_batch_restore(wlg_batch* b);
+/* measure every configuration (synchronous); results via wlg_batch_result */
+int wlg_batch_run(wlg_batch* b);
+int wlg_batch_result(wlg_batch* b, int i, double* wl_mat);
+/* device time of the last run and kernels per run */
+int wlg_batch_stats(wlg_batch* b, double* last_ms, int* kernels_per_run);
+void* wlg_batch_stream(wlg_batch* b);
+/* contraction shape for the whole batch (0 = automatic); G <= 4 */
+int wlg_batch_set_contract_shape(wlg_batch* b, int G, int SB, int nCB, int block);
+/* on (default): the first run executes directly and captures the pipeline,
+ * later runs replay the graph; off: every run executes directly */
+int wlg_batch_use_graph(wlg_batch* b, int on);
+/* device bytes a batch of these configurations would hold, or -1 */
+long long wlg_batch_estimate_bytes(int nconf, const int* dims, const int* bcs,
+                                   const wlg_wloop_parms* parms, int precision);
+
+/* ---- serving: a request loop with continuous batching -----------------------
+ * No counterpart in the reference.  Requests queue FIFO; max_inflight worker
+ * threads each take the oldest request plus pending requests of the same
+ * lattice and precision (up to max_batch) whose device footprint fits the
+ * budget (mem_fraction of the HBM free at creation, minus batches in flight)
+ * and the memory free now, and measure them as one wlg_batch on their own
+ * stream, so batches of different workers overlap on the device and new
+ * requests are admitted as soon as a worker and memory free up. */
+typedef struct {
+  int n[4];
+  int bc;
+  wlg_wloop_parms parms;  /* alpha_action: HYP of the gauge field, as wlg_measure */
+  int precision;          /* WLG_FP64 or WLG_MIXED */
+  uint64_t seed;          /* synthetic field (wlg_generate_links) when links == NULL */
+  double eps;
+  const double* links;    /* optional host AoS su3_dble field, copied at submission */
+} wlg_request;
+typedef struct wlg_server wlg_server;
+int wlg_server_create(int device, double mem_fraction, int max_inflight, int max_batch,
+                      wlg_server** out);
+int wlg_server_destroy(wlg_server* s);
+/* returns the request id (> 0) or -1 */
+long long wlg_server_submit(wlg_server* s, const wlg_request* r);
+/* blocks until request id is done; wl_mat (may be NULL) gets its result */
+int wlg_server_wait(wlg_server* s, long long id, double* wl_mat, double* latency_ms,
+                    int* batch_size);
+int wlg_server_release(wlg_server* s, long long id);
+const char* wlg_server_error(void);
+/* latency percentiles over completed requests (submission to result on the
+ * host) and completed requests per second since the first submission */
+int wlg_server_stats(wlg_server* s, long long* completed, long long* failed, long long* batches,
+                     double* p50_ms, double* p99_ms, double* throughput);
+long long wlg_server_budget(wlg_server* s);
+
 /* ---- plaquette sum without device allocation -------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory at this point (memory owned by another allocator or a preallocated
@@ -163,8 +233,8 @@ int wlg_reset_kernel_times(wlg_ctx* ctx);
  * per thread (1,2,3,4,6), nCB column blocks per (x0, level group), block
  * threads (multiple of 32, at most 128). */
 int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
-/* As above plus the kernel form (1 or 2) and SB top levels per reduction
- * (1 or 2). */
+/* As above plus the kernel form (2: register-prefetching, 3: staged top
+ * lines) and SB top levels per reduction (1 or 2). */
 int wlg_set_contract_tuning(wlg_ctx* ctx, int variant, int G, int SB, int nCB, int block);
 /* The context's CUDA stream (cudaStream_t), for callers that record events. */
 void* wlg_stream(wlg_ctx* ctx);

@@ -1,0 +1,110 @@
+"""Batches (wlg_batch): many configurations of different lattices measured
+in one CUDA-graph launch must give, configuration by configuration, what one
+context gives for each alone (the batched kernels run the same per-lattice
+arithmetic and the same reduction order: results are identical), and the
+FP64 batch matches the oracle."""
+import numpy as np
+import pytest
+
+from tests import oracle as O
+from wloop_b200 import APE, HYP, Context, WloopParms, generate_links
+from wloop_b200.api import Batch
+from wloop_b200.autotune import candidates
+from wloop_b200.workloads import batch_workloads, flops_per_config
+
+ITEMS = [
+    ((8, 4, 4, 4), 3, WloopParms(msl=3, nss=[0, 1, 2], mwlt=3, mwlr=2, op_smear=APE, alpha_ape=0.5,
+                                 proj_iter=4)),
+    ((6, 4, 6, 4), 0, WloopParms(msl=3, nss=[1, 0, 2], mwlt=3, mwlr=3, op_smear=APE, alpha_ape=0.4,
+                                 proj_iter=3)),
+    ((8, 6, 4, 4), 3, WloopParms(msl=2, nss=[0, 2], mwlt=4, mwlr=2, op_smear=HYP,
+                                 alpha_hyp=(0.75, 0.3), proj_iter=4)),
+    ((4, 4, 4, 4), 0, WloopParms(msl=4, nss=[0, 1, 1, 1], mwlt=2, mwlr=3, op_smear=APE,
+                                 alpha_ape=0.5, proj_iter=0)),
+]
+
+
+def test_batch_workloads_definition():
+    ws = batch_workloads()
+    assert len(ws) == 64
+    assert sum(1 for w in ws if w.n == (32, 16, 16, 16)) == 48
+    assert sum(1 for w in ws if w.n == (48, 24, 24, 24)) == 16
+    assert all(0.15 <= w.eps <= 0.35 for w in ws)
+    assert all(w.parms.mwlr == w.n[1] // 2 and w.parms.mwlt == w.n[1] // 2 for w in ws)
+    assert len({w.seed for w in ws}) == 64
+    assert flops_per_config(ws[0])["total"] > 0
+
+
+def test_autotune_candidates():
+    assert all(G <= 4 for G, _, _, _ in candidates(4, False, True))
+    assert (6, 1, 64, 0) in candidates(6, False, False)
+    assert all(G <= 3 and b == 64 for G, _, b, _ in candidates(6, True, False))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_batch_equals_single_contexts(prec):
+    fields = [generate_links(n, bc, 300 + i, 0.3) for i, (n, bc, _) in enumerate(ITEMS)]
+    singles = []
+    for (n, bc, p), u in zip(ITEMS, fields):
+        with Context(n, bc, prec) as c:
+            c.upload(u)
+            singles.append(c.measure(p))
+    with Batch(ITEMS, prec) as b:
+        for i, u in enumerate(fields):
+            b.upload(i, u)
+        b.snapshot()
+        b.run()
+        first = [b.result(i) for i in range(len(ITEMS))]
+        b.restore()
+        b.run()  # graph replay
+        for i in range(len(ITEMS)):
+            assert np.array_equal(first[i], singles[i]), f"config {i}"
+            assert np.array_equal(b.result(i), singles[i]), f"config {i} (replay)"
+        # new field in one slot: only that configuration changes
+        u2 = generate_links(ITEMS[1][0], ITEMS[1][1], 999, 0.3)
+        b.restore()
+        b.upload(1, u2)
+        b.run()
+        with Context(ITEMS[1][0], ITEMS[1][1], prec) as c:
+            c.upload(u2)
+            ref1 = c.measure(ITEMS[1][2])
+        assert np.array_equal(b.result(1), ref1)
+        assert np.array_equal(b.result(0), singles[0])
+        ms, kernels = b.stats()
+        assert ms > 0 and kernels > 0
+
+
+@pytest.mark.gpu
+def test_batch_fp64_matches_oracle():
+    fields = [generate_links(n, bc, 500 + i, 0.25) for i, (n, bc, _) in enumerate(ITEMS)]
+    with Batch(ITEMS, "fp64") as b:
+        for i, u in enumerate(fields):
+            b.upload(i, u)
+        b.run()
+        for i, ((n, bc, p), u) in enumerate(zip(ITEMS, fields)):
+            uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
+            ref, ref_abs = O.wloop_sum(n, bc, uh, p, want_abs=True)
+            got = b.result(i)
+            zero = ref == 0.0
+            assert np.all(got[zero] == 0.0)
+            err = np.abs(got - ref)[~zero] / np.maximum(np.abs(ref), ref_abs)[~zero]
+            assert err.max() <= 1e-12
+
+
+@pytest.mark.gpu
+def test_batch_generate_and_shape_change():
+    items = ITEMS[:2]
+    with Batch(items, "mixed") as b:
+        b.generate([7, 8], [0.2, 0.3])
+        b.snapshot()
+        b.run()
+        r0 = [b.result(i) for i in range(2)]
+        b.set_contract_shape(G=1, SB=1, nCB=0, block=64)
+        b.restore()
+        b.run()
+        for i in range(2):
+            assert np.abs(b.result(i) - r0[i]).max() < 1e-12
+        with Context(items[0][0], items[0][1], "mixed") as c:
+            c.generate(7, 0.2)
+            assert np.array_equal(c.measure(items[0][2]), r0[0])

@@ -1,0 +1,85 @@
+"""Serving loop (wlg_server): continuous batching of measurement requests.
+
+The result of a request is identical alone and in a mix of concurrent
+requests of other lattices (same per-lattice arithmetic and reduction order
+in every batch), and identical to a context's wlg_measure on the same field;
+requests that cannot fit the memory budget fail with a message instead of
+blocking the queue.
+"""
+import time
+
+import numpy as np
+import pytest
+
+from wloop_b200 import APE, Context, WloopParms, generate_links
+from wloop_b200.api import Server, estimate_bytes
+
+P = WloopParms(msl=3, nss=[0, 2, 2], mwlt=3, mwlr=2, op_smear=APE, alpha_ape=0.5, proj_iter=4)
+
+
+def test_estimate_bytes_scales_with_volume():
+    a = estimate_bytes((8, 4, 4, 4), 3, P, "mixed")
+    b = estimate_bytes((16, 8, 8, 8), 3, P, "mixed")
+    c = estimate_bytes((16, 8, 8, 8), 3, P, "fp64")
+    assert 0 < a < b < c
+    assert b > 8 * a
+
+
+@pytest.mark.gpu
+def test_result_same_alone_and_in_mix():
+    x = ((8, 4, 4, 4), 3, 4711, 0.25)
+    with Server(max_inflight=2, max_batch=4) as s:
+        rid = s.submit(x[0], x[1], P, "mixed", seed=x[2], eps=x[3])
+        alone, lat, bs = s.wait(rid)
+        assert bs == 1 and lat > 0
+    others = [((6, 4, 6, 4), 0, 11, 0.3), ((8, 4, 4, 4), 0, 12, 0.2), ((8, 4, 4, 4), 3, 13, 0.3),
+              ((12, 6, 6, 6), 3, 14, 0.2), ((8, 4, 4, 4), 3, 15, 0.35)]
+    with Server(max_inflight=3, max_batch=4) as s:
+        ids = []
+        for k, o in enumerate(others):
+            ids.append(s.submit(o[0], o[1], P, "mixed", seed=o[2], eps=o[3]))
+            if k == 1:
+                mine = s.submit(x[0], x[1], P, "mixed", seed=x[2], eps=x[3])
+        mixed_res, _, bs_mix = s.wait(mine)
+        outs = [s.wait(i) for i in ids]
+        st = s.stats()
+    assert np.array_equal(alone, mixed_res), "result differs alone vs in the mix"
+    assert st["completed"] == len(others) + 1 and st["failed"] == 0
+    assert st["p99_ms"] >= st["p50_ms"] > 0
+    # every result equals a plain context measurement of the same field
+    for o, (res, _, _) in zip(others, outs):
+        with Context(o[0], o[1], "mixed") as c:
+            c.generate(o[2], o[3])
+            assert np.array_equal(c.measure(P), res)
+
+
+@pytest.mark.gpu
+def test_host_field_request_matches_context():
+    n, bc = (8, 6, 4, 4), 0
+    u = generate_links(n, bc, 99, 0.3)
+    with Server(max_inflight=1) as s:
+        res, _, _ = s.wait(s.submit(n, bc, P, "fp64", links=u))
+    with Context(n, bc, "fp64") as c:
+        c.upload(u)
+        assert np.array_equal(c.measure(P), res)
+
+
+@pytest.mark.gpu
+def test_request_over_budget_fails_cleanly():
+    with Server(mem_fraction=1e-6, max_inflight=1) as s:
+        rid = s.submit((8, 4, 4, 4), 3, P, "mixed", seed=1)
+        with pytest.raises(Exception, match="budget"):
+            s.wait(rid)
+        assert s.stats()["failed"] == 1
+
+
+@pytest.mark.gpu
+def test_requests_overlap_and_batch():
+    with Server(max_inflight=2, max_batch=8) as s:
+        t0 = time.time()
+        ids = [s.submit((8, 4, 4, 4), 3, P, "mixed", seed=100 + i, eps=0.2) for i in range(12)]
+        res = [s.wait(i) for i in ids]
+        st = s.stats()
+    assert st["completed"] == 12
+    assert st["batches"] < 12  # requests that queued together were measured together
+    assert max(bs for _, _, bs in res) > 1

@@ -33,6 +33,19 @@ class WlgParms(C.Structure):
     ]
 
 
+class WlgRequest(C.Structure):
+    """Mirror of wlg_request (include/wloop_b200.h)."""
+    _fields_ = [
+        ("n", C.c_int * 4),
+        ("bc", C.c_int),
+        ("parms", WlgParms),
+        ("precision", C.c_int),
+        ("seed", C.c_uint64),
+        ("eps", C.c_double),
+        ("links", C.POINTER(C.c_double)),
+    ]
+
+
 class WlgError(RuntimeError):
     pass
 
@@ -79,6 +92,31 @@ def _load():
         "wlg_snapshot": (i, [vp]),
         "wlg_restore": (i, [vp]),
         "wlg_peak_flops": (i, [i, i, dp]),
+        "wlg_batch_create": (i, [i, ip, ip, C.POINTER(WlgParms), i, i, C.POINTER(vp)]),
+        "wlg_batch_destroy": (i, [vp]),
+        "wlg_batch_size": (i, [vp]),
+        "wlg_batch_bytes": (C.c_longlong, [vp]),
+        "wlg_batch_upload": (i, [vp, i, dp]),
+        "wlg_batch_generate": (i, [vp, C.POINTER(u64), dp]),
+        "wlg_batch_snapshot": (i, [vp]),
+        "wlg_batch_restore": (i, [vp]),
+        "wlg_batch_run": (i, [vp]),
+        "wlg_batch_result": (i, [vp, i, dp]),
+        "wlg_batch_stats": (i, [vp, dp, ip]),
+        "wlg_batch_stream": (vp, [vp]),
+        "wlg_batch_set_contract_shape": (i, [vp, i, i, i, i]),
+        "wlg_plaq_sum_noalloc": (i, [vp, ip, i, vp, vp]),
+        "wlg_batch_use_graph": (i, [vp, i]),
+        "wlg_batch_estimate_bytes": (C.c_longlong, [i, ip, ip, C.POINTER(WlgParms), i]),
+        "wlg_server_create": (i, [i, d, i, i, C.POINTER(vp)]),
+        "wlg_server_destroy": (i, [vp]),
+        "wlg_server_submit": (C.c_longlong, [vp, C.POINTER(WlgRequest)]),
+        "wlg_server_wait": (i, [vp, C.c_longlong, dp, dp, ip]),
+        "wlg_server_release": (i, [vp, C.c_longlong]),
+        "wlg_server_error": (C.c_char_p, []),
+        "wlg_server_stats": (i, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                 C.POINTER(C.c_longlong), dp, dp, dp]),
+        "wlg_server_budget": (C.c_longlong, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

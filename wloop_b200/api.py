@@ -17,7 +17,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from ._native import (WLG_FP64, WLG_MAX_SM_LEVELS, WLG_MIXED, WLG_OP_APE, WLG_OP_HYP, WlgError,
-                      WlgParms, check, dptr, iptr, lib)
+                      WlgParms, WlgRequest, check, dptr, iptr, lib)
 
 APE, HYP = WLG_OP_APE, WLG_OP_HYP
 PRECISIONS = {"fp64": WLG_FP64, "mixed": WLG_MIXED}
@@ -265,3 +265,160 @@ def approx_project_to_su3(m: np.ndarray, iterations: int) -> None:
     """approx_project_to_su3_dble (projection.c:120-154) in place on (..., 3, 3)."""
     assert m.flags.c_contiguous and m.dtype == np.complex128
     check(lib.wlg_project(dptr(m.view(np.float64)), m.size // 9, iterations), "project")
+
+
+class Batch:
+    """Many configurations measured together (wlg_batch): every stage is one
+    kernel over all lattices and the pipeline replays as one CUDA graph."""
+
+    def __init__(self, items, precision: str = "mixed", device: int = 0):
+        """items: sequence of (n, bc, WloopParms)."""
+        self.items = [(tuple(int(x) for x in n), int(bc), p) for n, bc, p in items]
+        k = len(self.items)
+        dims = np.asarray([n for n, _, _ in self.items], dtype=np.int32).reshape(-1)
+        bcs = np.asarray([bc for _, bc, _ in self.items], dtype=np.int32)
+        parr = (WlgParms * k)(*[p.to_c() for _, _, p in self.items])
+        h = C.c_void_p()
+        check(lib.wlg_batch_create(k, iptr(dims), iptr(bcs), parr, PRECISIONS[precision], device,
+                                   C.byref(h)), "batch_create")
+        self._h = h
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.wlg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __len__(self):
+        return len(self.items)
+
+    @property
+    def device_bytes(self) -> int:
+        return lib.wlg_batch_bytes(self._h)
+
+    def upload(self, i: int, u: np.ndarray):
+        u = np.ascontiguousarray(u, dtype=np.complex128)
+        check(lib.wlg_batch_upload(self._h, i, dptr(u.view(np.float64))), "batch_upload")
+
+    def generate(self, seeds, eps):
+        s = (C.c_uint64 * len(self.items))(*[int(x) for x in seeds])
+        e = np.ascontiguousarray(eps, dtype=np.float64)
+        check(lib.wlg_batch_generate(self._h, s, dptr(e)), "batch_generate")
+
+    def snapshot(self):
+        check(lib.wlg_batch_snapshot(self._h), "batch_snapshot")
+
+    def restore(self):
+        check(lib.wlg_batch_restore(self._h), "batch_restore")
+
+    def run(self):
+        check(lib.wlg_batch_run(self._h), "batch_run")
+
+    def result(self, i: int) -> np.ndarray:
+        n, _, p = self.items[i]
+        out = np.empty(p.wls(n[0]))
+        check(lib.wlg_batch_result(self._h, i, dptr(out)), "batch_result")
+        return out
+
+    def stats(self):
+        ms = C.c_double()
+        k = C.c_int()
+        check(lib.wlg_batch_stats(self._h, C.byref(ms), C.byref(k)), "batch_stats")
+        return ms.value, k.value
+
+    @property
+    def stream(self) -> int:
+        return lib.wlg_batch_stream(self._h) or 0
+
+    def set_contract_shape(self, G=0, SB=0, nCB=0, block=0):
+        check(lib.wlg_batch_set_contract_shape(self._h, G, SB, nCB, block),
+              "batch_set_contract_shape")
+
+
+def estimate_bytes(n, bc: int, p: WloopParms, precision: str = "mixed") -> int:
+    """Device bytes one measurement of this lattice holds in a batch."""
+    nn = np.asarray(n, dtype=np.int32)
+    b = np.asarray([bc], dtype=np.int32)
+    cp = p.to_c()
+    return int(lib.wlg_batch_estimate_bytes(1, iptr(nn), iptr(b), C.byref(cp), PRECISIONS[precision]))
+
+
+class Server:
+    """Measurement request loop with continuous batching (wlg_server)."""
+
+    def __init__(self, device: int = 0, mem_fraction: float = 0.8, max_inflight: int = 2,
+                 max_batch: int = 8):
+        h = C.c_void_p()
+        if lib.wlg_server_create(device, mem_fraction, max_inflight, max_batch, C.byref(h)) != 0:
+            raise WlgError("server_create failed (no device or bad arguments)")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.wlg_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def budget(self) -> int:
+        return int(lib.wlg_server_budget(self._h))
+
+    def submit(self, n, bc: int, p: WloopParms, precision: str = "mixed", seed: int = 0,
+               eps: float = 0.2, links: Optional[np.ndarray] = None) -> int:
+        r = WlgRequest()
+        for i in range(4):
+            r.n[i] = int(n[i])
+        r.bc = bc
+        r.parms = p.to_c()
+        r.precision = PRECISIONS[precision]
+        r.seed = int(seed)
+        r.eps = float(eps)
+        if links is not None:
+            links = np.ascontiguousarray(links, dtype=np.complex128)
+            r.links = dptr(links.view(np.float64))
+        rid = lib.wlg_server_submit(self._h, C.byref(r))
+        if rid < 0:
+            raise WlgError("server_submit: bad request")
+        self._nwl = getattr(self, "_nwl", {})
+        self._nwl[rid] = p.wls(int(n[0]))
+        return rid
+
+    def wait(self, rid: int):
+        out = np.empty(self._nwl[rid])
+        lat = C.c_double()
+        bs = C.c_int()
+        if lib.wlg_server_wait(self._h, rid, dptr(out), C.byref(lat), C.byref(bs)) != 0:
+            raise WlgError("request %d failed: %s" % (rid, lib.wlg_server_error().decode()))
+        lib.wlg_server_release(self._h, rid)
+        return out, lat.value, bs.value
+
+    def stats(self) -> dict:
+        c, f, b = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        p50, p99, thr = C.c_double(), C.c_double(), C.c_double()
+        check(lib.wlg_server_stats(self._h, C.byref(c), C.byref(f), C.byref(b), C.byref(p50),
+                                   C.byref(p99), C.byref(thr)), "server_stats")
+        return {"completed": c.value, "failed": f.value, "batches": b.value,
+                "p50_ms": p50.value, "p99_ms": p99.value, "throughput": thr.value}

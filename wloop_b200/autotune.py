@@ -1,0 +1,138 @@
+"""Autotuner for the contraction kernel's shape (the dominant kernel).
+
+A shape is (G bottom levels per thread, SB top levels per reduction, threads
+per block, column blocks per (x0, level group)).  The tuner times every
+candidate on the caller's own data -- a Context (one lattice) or a Batch
+(many) -- through the C ABI, keeps the fastest, and caches it on disk keyed by
+precision, lattices and loop parameters, so later runs of the same workload
+start from the tuned shape.  Cache: $WLG_TUNE_CACHE or
+~/.cache/wloop_b200/contract_tune.json.
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+from typing import Dict, List, Optional, Sequence, Tuple
+
+Shape = Tuple[int, int, int, int]  # (G, SB, block, nCB)
+
+
+def cache_path() -> str:
+    p = os.environ.get("WLG_TUNE_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "wloop_b200", "contract_tune.json")
+
+
+def _load() -> Dict[str, list]:
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(key: str, shape: Shape) -> None:
+    d = _load()
+    d[key] = list(shape)
+    p = cache_path()
+    os.makedirs(os.path.dirname(p), exist_ok=True)
+    tmp = p + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+    os.replace(tmp, p)
+
+
+def candidates(msl: int, fp64: bool, batched: bool) -> List[Shape]:
+    """Shapes worth timing for msl levels."""
+    out: List[Shape] = []
+    gs = [g for g in (1, 2, 3, 4) if g <= msl]
+    if not batched and not fp64 and msl == 6:
+        gs.append(6)
+    for G in gs:
+        if fp64 and G > 3:
+            continue
+        for SB in (1, 2):
+            if G == 6 and SB == 2:
+                continue
+            for block in ((64,) if fp64 else (64, 128)):
+                out.append((G, SB, block, 0))
+    return out
+
+
+def key_for(precision: str, lattices: Sequence[tuple], parms) -> str:
+    lat = ";".join("x".join(str(v) for v in n) for n in lattices)
+    return f"{precision}|{lat}|msl{parms.msl}|t{parms.mwlt}|r{parms.mwlr}"
+
+
+def cached(key: str) -> Optional[Shape]:
+    v = _load().get(key)
+    return tuple(v) if v else None
+
+
+def tune_context(ctx, parms, precision: str, reps: int = 1, use_cache: bool = True) -> Shape:
+    """Times the contraction of a Context on its current field (the field is
+    restored from a snapshot before every run) and applies the best shape."""
+    key = key_for(precision, [ctx.n], parms)
+    if use_cache and cached(key):
+        G, SB, block, nCB = cached(key)
+        ctx.set_contract_tuning(3 if G <= 4 else 2, G, SB, nCB, block)
+        return cached(key)
+    ctx.snapshot()
+    best, best_t = None, float("inf")
+    for (G, SB, block, nCB) in candidates(parms.msl, precision == "fp64", batched=False):
+        ctx.set_contract_tuning(3 if G <= 4 else 2, G, SB, nCB, block)
+        ctx.restore()
+        ctx.measure(parms)  # warm-up
+        ctx.reset_kernel_times()
+        ctx.set_profiling(True)
+        for _ in range(reps):
+            ctx.restore()
+            ctx.measure(parms)
+        ms, n = ctx.kernel_time("contract")
+        ctx.set_profiling(False)
+        t = ms / max(1, n)
+        if t < best_t:
+            best, best_t = (G, SB, block, nCB), t
+    G, SB, block, nCB = best
+    ctx.set_contract_tuning(3 if G <= 4 else 2, G, SB, nCB, block)
+    ctx.restore()
+    _store(key, best)
+    return best
+
+
+def tune_batch(batch, reps: int = 1, use_cache: bool = True) -> Shape:
+    """Times whole batch runs (one CUDA-graph launch each) per candidate and
+    applies the best shape.  The batch's fields are restored from a snapshot
+    before every run."""
+    lat = [n for n, _, _ in batch.items]
+    p0 = batch.items[0][2]
+    key = key_for(batch.precision, lat, p0)
+    if use_cache and cached(key):
+        batch.set_contract_shape(*_as_batch(cached(key)))
+        return cached(key)
+    msl = max(p.msl for _, _, p in batch.items)
+    batch.snapshot()
+    best, best_t = None, float("inf")
+    for shape in candidates(msl, batch.precision == "fp64", batched=True):
+        batch.set_contract_shape(*_as_batch(shape))
+        batch.restore()
+        batch.run()  # builds and captures the graph
+        t = 0.0
+        for _ in range(reps):
+            batch.restore()
+            batch.run()
+            t += batch.stats()[0]
+        t /= reps
+        if t < best_t:
+            best, best_t = shape, t
+    batch.set_contract_shape(*_as_batch(best))
+    batch.restore()
+    _store(key, best)
+    return best
+
+
+def _as_batch(shape: Shape):
+    G, SB, block, nCB = shape
+    return G, SB, nCB, block

@@ -1,0 +1,737 @@
+// batch.cu -- many configurations, of possibly different lattices, measured
+// together: every stage is one kernel over the flattened work of all
+// lattices (the batched kernels of smear.cu / loops.cu), and the whole
+// pipeline -- HYP, the spatial smearing levels, and for every spatial extent
+// the line step, the contraction and its reduction, then the result copies --
+// is captured once into a CUDA graph and replayed per batch.
+//
+// Memory: one arena per batch.  Per lattice: the gauge field, its snapshot,
+// and one region that holds the HYP scratch while HYP runs and afterwards the
+// APE ping-pong buffers, the level store and the spatial lines (HYP has
+// finished for every lattice before the first sweep writes there).
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "internal.h"
+#include "../../include/wloop_b200.h"
+
+using namespace wlg;
+
+namespace {
+
+struct Cfg {
+  Geo g;
+  int bc;
+  wlg_wloop_parms p;
+  ContractPlan cp;
+  size_t D;  // elements per direction array
+  size_t U, U0, region, wl;  // byte offsets in the arena
+  size_t partial;            // byte offset in the partial-sum buffer
+  size_t nwl;
+  size_t wl_host;  // offset (doubles) in the pinned result block
+};
+
+enum OpKind { OP_SMEAR, OP_COPY, OP_LINES, OP_CONTRACT, OP_REDUCE, OP_D2H };
+
+struct Op {
+  int kind;
+  int stage;           // OP_SMEAR
+  size_t tab, pre;     // byte offsets of the argument table and prefix in the table buffer
+  int n;               // lattices in the launch
+  long long total;     // work items (blocks for OP_CONTRACT)
+  int G, SB, block;    // OP_CONTRACT
+  size_t smem;
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+struct wlg_batch {
+  int dev = 0, prec = WLG_FP64;
+  cudaStream_t st = nullptr;
+  std::vector<Cfg> cfg;
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  char* pbuf = nullptr;  // contraction partial sums (depends on the contraction plan)
+  size_t pbuf_bytes = 0, pbuf_cap = 0;
+  char* tables = nullptr;
+  double* wl_host = nullptr;  // pinned
+  size_t wl_host_doubles = 0;
+  char* staging = nullptr;    // device AoS staging for uploads
+  size_t staging_bytes = 0;
+  std::vector<Op> ops;
+  std::vector<char> host_tables;
+  bool built = false;      // argument tables on the device
+  bool use_graph = true;   // capture the pipeline after the first run and replay it
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int tG = 0, tSB = 0, tBlock = 0, tNCB = 0;  // contraction shape override (tuning)
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  int kernels = 0;
+};
+
+namespace {
+
+size_t elem_bytes(const wlg_batch* b) { return b->prec == WLG_FP64 ? sizeof(double2) : sizeof(float2); }
+
+template <class T> Links<T> lview(char* base, size_t D, int ndir, int first_mu) {
+  Links<T> L;
+  typename V2<T>::t* p = (typename V2<T>::t*)base;
+  for (int mu = 0; mu < 4; mu++) L.p[mu] = nullptr;
+  for (int k = 0; k < ndir; k++) L.p[first_mu + k] = p + (size_t)k * D;
+  return L;
+}
+
+int check_parms(const Geo& g, const wlg_wloop_parms& p) {
+  if (p.msl < 1 || p.msl > WLG_MAX_SM_LEVELS) return -1;
+  if (p.mwlt < 1 || p.mwlt > g.n[0] / 2 + 1) return -1;
+  if (p.mwlr < 1 || p.mwlr > g.n[1] / 2 + 1 || p.mwlr > g.n[2] / 2 + 1 || p.mwlr > g.n[3] / 2 + 1)
+    return -1;
+  if (p.op_smear != WLG_OP_APE && p.op_smear != WLG_OP_HYP) return -1;
+  for (int i = 0; i < p.msl; i++)
+    if (p.nss[i] < 0) return -1;
+  return 0;
+}
+
+// ---- table builder ----------------------------------------------------------
+struct Tables {
+  std::vector<char> bytes;
+  template <class R> size_t add(const std::vector<R>& recs) {
+    size_t off = align256(bytes.size());
+    bytes.resize(off + recs.size() * sizeof(R));
+    memcpy(bytes.data() + off, recs.data(), recs.size() * sizeof(R));
+    return off;
+  }
+  size_t add_prefix(const std::vector<long long>& units) {
+    std::vector<long long> pre(units.size() + 1, 0);
+    for (size_t i = 0; i < units.size(); i++) pre[i + 1] = pre[i] + units[i];
+    return add(pre);
+  }
+};
+
+template <class T> void build_ops(wlg_batch* b) {
+  typedef typename V2<T>::t T2;
+  Tables tb;
+  b->ops.clear();
+  const int n = (int)b->cfg.size();
+  auto base = [&](size_t off) { return b->arena + off; };
+  auto push_smear = [&](int stage, const std::vector<SArgs<T>>& A, const std::vector<long long>& u) {
+    if (A.empty()) return;
+    Op op{};
+    op.kind = OP_SMEAR;
+    op.stage = stage;
+    op.tab = tb.add(A);
+    op.pre = tb.add_prefix(u);
+    op.n = (int)A.size();
+    op.total = 0;
+    for (long long x : u) op.total += x;
+    b->ops.push_back(op);
+  };
+  auto push_copy = [&](void* dst, const void* src, size_t bytes) {
+    Op op{};
+    op.kind = OP_COPY;
+    op.dst = dst;
+    op.src = src;
+    op.bytes = bytes;
+    b->ops.push_back(op);
+  };
+
+  // ---- HYP (hyp_links, all directions) ----
+  {
+    std::vector<SArgs<T>> a3, a2, a1;
+    std::vector<long long> u12, u4;
+    for (int c = 0; c < n; c++) {
+      const Cfg& f = b->cfg[c];
+      if (f.p.alpha_action[0] == 0.0) continue;  // hyp_links.c:405
+      SArgs<T> A;
+      memset(&A, 0, sizeof(A));
+      A.g = f.g;
+      A.U = lview<T>(base(f.U), f.D, 4, 0);
+      A.aux0 = (T2*)base(f.region);
+      A.aux1 = (T2*)base(f.region) + 12 * f.D;
+      A.proj = f.p.proj_iter > 0;
+      A.iter = f.p.proj_iter;
+      A.bc = f.bc;
+      A.mu0 = 0;
+      A.nmu = 4;
+      SArgs<T> x = A;
+      x.a = 1.0 - f.p.alpha_action[2];
+      x.b = f.p.alpha_action[2] / 2.0;
+      a3.push_back(x);
+      x.a = 1.0 - f.p.alpha_action[1];
+      x.b = f.p.alpha_action[1] / 4.0;
+      a2.push_back(x);
+      x.a = 1.0 - f.p.alpha_action[0];
+      x.b = f.p.alpha_action[0] / 6.0;
+      a1.push_back(x);
+      u12.push_back(12LL * f.g.vol);
+      u4.push_back(4LL * f.g.vol);
+    }
+    push_smear(BATCH_HYP3, a3, u12);
+    push_smear(BATCH_HYP2, a2, u12);
+    push_smear(BATCH_HYP1, a1, u4);
+  }
+
+  // ---- spatial smearing levels (smear.c:99-121) ----
+  // per lattice: cur = spatial links of U; sweep i of level sl writes the
+  // level slot on its last sweep, else the ping-pong buffer not holding cur
+  std::vector<Links<T>> cur(n), A(n), B(n);
+  std::vector<char*> levels(n), lines(n), dl(n);
+  int maxmsl = 0, maxr = 0;
+  for (int c = 0; c < n; c++) {
+    const Cfg& f = b->cfg[c];
+    char* r = base(f.region);
+    size_t es = elem_bytes(b);
+    A[c] = lview<T>(r, f.D, 3, 1);
+    B[c] = lview<T>(r + 3 * f.D * es, f.D, 3, 1);
+    levels[c] = r + 6 * f.D * es;
+    lines[c] = r + (6 + 3 * (size_t)f.p.msl) * f.D * es;
+    dl[c] = r + (6 + 6 * (size_t)f.p.msl) * f.D * es;
+    cur[c] = lview<T>(base(f.U) + f.D * es, f.D, 3, 1);
+    maxmsl = std::max(maxmsl, f.p.msl);
+    maxr = std::max(maxr, f.p.mwlr);
+  }
+  for (int sl = 0; sl < maxmsl; sl++) {
+    int maxns = 0;
+    for (int c = 0; c < n; c++) {
+      const Cfg& f = b->cfg[c];
+      if (sl >= f.p.msl) continue;
+      maxns = std::max(maxns, f.p.nss[sl]);
+      if (f.p.nss[sl] == 0) {
+        Links<T> lv = lview<T>(levels[c] + (size_t)sl * 3 * f.D * elem_bytes(b), f.D, 3, 1);
+        for (int k = 1; k < 4; k++) push_copy(lv.p[k], cur[c].p[k], f.D * elem_bytes(b));
+        cur[c] = lv;
+      }
+    }
+    for (int i = 0; i < maxns; i++) {
+      std::vector<SArgs<T>> ape, h1, h2;
+      std::vector<long long> u3, u6;
+      for (int c = 0; c < n; c++) {
+        const Cfg& f = b->cfg[c];
+        if (sl >= f.p.msl || i >= f.p.nss[sl]) continue;
+        Links<T> lv = lview<T>(levels[c] + (size_t)sl * 3 * f.D * elem_bytes(b), f.D, 3, 1);
+        Links<T> dst = (i == f.p.nss[sl] - 1) ? lv : ((cur[c].p[1] == A[c].p[1]) ? B[c] : A[c]);
+        SArgs<T> x;
+        memset(&x, 0, sizeof(x));
+        x.g = f.g;
+        x.proj = f.p.proj_iter > 0;
+        x.iter = f.p.proj_iter;
+        if (f.p.op_smear == WLG_OP_APE) {
+          x.U = cur[c];
+          x.D = dst;
+          x.a = f.p.alpha_ape;
+          x.mu0 = 1;
+          ape.push_back(x);
+          u3.push_back(3LL * f.g.vol);
+        } else {
+          // spatial HYP: level 1 from cur into dl, copy cur -> dst, level 2 in place on dst
+          x.U = cur[c];
+          x.aux0 = (T2*)dl[c];
+          x.a = 1.0 - f.p.alpha_hyp[1];
+          x.b = f.p.alpha_hyp[1] / 2.0;
+          h1.push_back(x);
+          u6.push_back(6LL * f.g.vol);
+          x.D = dst;
+          x.a = 1.0 - f.p.alpha_hyp[0];
+          x.b = f.p.alpha_hyp[0] / 4.0;
+          h2.push_back(x);
+        }
+        cur[c] = dst;
+      }
+      push_smear(BATCH_APE, ape, u3);
+      if (!h1.empty()) {
+        push_smear(BATCH_HYP3D1, h1, u6);
+        std::vector<long long> u3h;
+        for (auto& x : h2) {
+          u3h.push_back(3LL * x.g.vol);
+          // the source of this sweep is h1's U for the same lattice
+        }
+        for (size_t j = 0; j < h2.size(); j++)
+          for (int k = 1; k < 4; k++)
+            if (h1[j].U.p[k] != h2[j].D.p[k])
+              push_copy(h2[j].D.p[k], h1[j].U.p[k], link_elems<T>(h2[j].g.vol) * elem_bytes(b));
+        push_smear(BATCH_HYP3D2, h2, u3h);
+      }
+    }
+  }
+
+  // ---- loops (wloop.c:524-608) ----
+  for (int r = 0; r < maxr; r++) {
+    const int R = r + 1;
+    std::vector<LArgs<T>> la;
+    std::vector<long long> lu;
+    std::vector<RArgs> ra;
+    std::vector<long long> ru;
+    struct Group {
+      int G, SB, block;
+      size_t smem;
+      std::vector<CArgs<T>> a;
+      std::vector<long long> blocks;
+    };
+    std::vector<Group> groups;
+    for (int c = 0; c < n; c++) {
+      const Cfg& f = b->cfg[c];
+      if (r >= f.p.mwlr) continue;
+      const T2* lev = (const T2*)levels[c];
+      const T2* L = lev;
+      if (R >= 2) {
+        LArgs<T> x;
+        x.g = f.g;
+        x.msl = f.p.msl;
+        x.R = R;
+        x.level = lev;
+        x.src = (R == 2) ? lev : (const T2*)lines[c];
+        x.dst = (T2*)lines[c];
+        la.push_back(x);
+        lu.push_back((long long)f.p.msl * 3 * f.g.vol);
+        L = (const T2*)lines[c];
+      }
+      CArgs<T> ca;
+      ca.g = f.g;
+      ca.u0 = (const T2*)base(f.U);
+      ca.lines = L;
+      ca.msl = f.p.msl;
+      ca.mwlt = f.p.mwlt;
+      ca.R = R;
+      ca.ngrp = f.cp.ngrp;
+      ca.nCB = f.cp.nCB;
+      ca.partial = (double*)(b->pbuf + f.partial);
+      Group* gp = nullptr;
+      for (auto& gr : groups)
+        if (gr.G == f.cp.G && gr.SB == f.cp.SB && gr.block == f.cp.block) gp = &gr;
+      if (!gp) {
+        groups.push_back(Group{f.cp.G, f.cp.SB, f.cp.block, 0, {}, {}});
+        gp = &groups.back();
+      }
+      gp->smem = std::max(gp->smem, contract3_smem<T>(f.cp, f.p.msl));
+      gp->a.push_back(ca);
+      gp->blocks.push_back((long long)f.g.n[0] * f.cp.ngrp * f.cp.nCB);
+      RArgs rr = reduce_args(f.g, f.cp, f.p.msl, f.p.mwlt, f.p.mwlr, r,
+                             (const double*)(b->pbuf + f.partial), (double*)base(f.wl));
+      ra.push_back(rr);
+      ru.push_back(rr.nout);
+    }
+    if (!la.empty()) {
+      Op op{};
+      op.kind = OP_LINES;
+      op.tab = tb.add(la);
+      op.pre = tb.add_prefix(lu);
+      op.n = (int)la.size();
+      for (long long x : lu) op.total += x;
+      b->ops.push_back(op);
+    }
+    for (auto& gr : groups) {
+      Op op{};
+      op.kind = OP_CONTRACT;
+      op.tab = tb.add(gr.a);
+      op.pre = tb.add_prefix(gr.blocks);
+      op.n = (int)gr.a.size();
+      for (long long x : gr.blocks) op.total += x;
+      op.G = gr.G;
+      op.SB = gr.SB;
+      op.block = gr.block;
+      op.smem = gr.smem;
+      b->ops.push_back(op);
+    }
+    if (!ra.empty()) {
+      Op op{};
+      op.kind = OP_REDUCE;
+      op.tab = tb.add(ra);
+      op.pre = tb.add_prefix(ru);
+      op.n = (int)ra.size();
+      for (long long x : ru) op.total += x;
+      b->ops.push_back(op);
+    }
+  }
+  for (int c = 0; c < n; c++) {
+    const Cfg& f = b->cfg[c];
+    Op op{};
+    op.kind = OP_D2H;
+    op.dst = b->wl_host + f.wl_host;
+    op.src = base(f.wl);
+    op.bytes = f.nwl * sizeof(double);
+    b->ops.push_back(op);
+  }
+  b->host_tables.swap(tb.bytes);
+}
+
+template <class T> int issue(wlg_batch* b) {
+  int kernels = 0;
+  for (const Op& op : b->ops) {
+    switch (op.kind) {
+      case OP_SMEAR:
+        smear_batch<T>(op.stage, (const SArgs<T>*)(b->tables + op.tab),
+                       (const long long*)(b->tables + op.pre), op.n, op.total, b->st);
+        kernels++;
+        break;
+      case OP_COPY:
+        WLG_CUDA(cudaMemcpyAsync(op.dst, op.src, op.bytes, cudaMemcpyDeviceToDevice, b->st));
+        break;
+      case OP_LINES:
+        line_step_batch<T>((const LArgs<T>*)(b->tables + op.tab),
+                           (const long long*)(b->tables + op.pre), op.n, op.total, b->st);
+        kernels++;
+        break;
+      case OP_CONTRACT:
+        contract_batch<T>(op.G, op.SB, (const CArgs<T>*)(b->tables + op.tab),
+                          (const long long*)(b->tables + op.pre), op.n, op.total, op.block,
+                          op.smem, b->st);
+        kernels++;
+        break;
+      case OP_REDUCE:
+        contract_reduce_batch((const RArgs*)(b->tables + op.tab),
+                              (const long long*)(b->tables + op.pre), op.n, op.total, b->st);
+        kernels++;
+        break;
+      case OP_D2H:
+        WLG_CUDA(cudaMemcpyAsync(op.dst, op.src, op.bytes, cudaMemcpyDeviceToHost, b->st));
+        break;
+    }
+  }
+  b->kernels = kernels;
+  return get_error()[0] ? -1 : 0;
+}
+
+// contraction plans and partial-sum offsets (may change with the shape)
+int plan(wlg_batch* b) {
+  size_t poff = 0;
+  const bool fp64 = b->prec == WLG_FP64;
+  for (Cfg& f : b->cfg) {
+    f.cp = contract_plan(f.g, f.p.msl, f.p.mwlt, fp64, b->tG, b->tNCB, b->tBlock);
+    if (b->tSB) f.cp.SB = b->tSB;
+    f.cp.variant = 3;
+    if (f.cp.G > 4) {
+      set_error("batch: contraction shape G=%d is not available in batched form", f.cp.G);
+      return -1;
+    }
+    f.partial = poff;
+    poff = align256(poff + f.cp.partial_doubles * sizeof(double));
+  }
+  b->pbuf_bytes = poff;
+  return 0;
+}
+
+// field offsets in the arena (fixed for the life of the batch)
+void layout(wlg_batch* b) {
+  size_t off = 0, host = 0, maxv = 0;
+  const bool fp64 = b->prec == WLG_FP64;
+  for (Cfg& f : b->cfg) {
+    f.D = fp64 ? link_elems<double>(f.g.vol) : link_elems<float>(f.g.vol);
+    size_t es = elem_bytes(b);
+    f.U = off;
+    off = align256(off + 4 * f.D * es);
+    f.U0 = off;
+    off = align256(off + 4 * f.D * es);
+    f.region = off;
+    size_t rdirs = std::max<size_t>(24, 12 + 6 * (size_t)f.p.msl);
+    off = align256(off + rdirs * f.D * es);
+    f.nwl = (size_t)f.p.msl * f.p.msl * f.p.mwlt * f.p.mwlr * f.g.n[0];
+    f.wl = off;
+    off = align256(off + f.nwl * sizeof(double));
+    f.wl_host = host;
+    host += f.nwl;
+    maxv = std::max(maxv, (size_t)f.g.vol);
+  }
+  b->arena_bytes = off;
+  b->wl_host_doubles = host;
+  b->staging_bytes = maxv * 4 * 144;
+}
+
+int ensure_pbuf(wlg_batch* b) {
+  if (b->pbuf && b->pbuf_cap >= b->pbuf_bytes) return 0;
+  if (b->pbuf) cudaFree(b->pbuf);
+  b->pbuf = nullptr;
+  b->pbuf_cap = 0;
+  if (cudaMalloc(&b->pbuf, std::max<size_t>(256, b->pbuf_bytes)) != cudaSuccess) {
+    set_error("batch: cannot allocate %zu bytes of partial sums", b->pbuf_bytes);
+    cudaGetLastError();
+    return -1;
+  }
+  b->pbuf_cap = std::max<size_t>(256, b->pbuf_bytes);
+  return 0;
+}
+
+int build(wlg_batch* b) {
+  if (b->built) return 0;
+  if (b->prec == WLG_FP64)
+    build_ops<double>(b);
+  else
+    build_ops<float>(b);
+  if (b->tables) cudaFree(b->tables);
+  b->tables = nullptr;
+  WLG_CUDA(cudaMalloc(&b->tables, std::max<size_t>(256, b->host_tables.size())));
+  WLG_CUDA(cudaMemcpy(b->tables, b->host_tables.data(), b->host_tables.size(),
+                      cudaMemcpyHostToDevice));
+  b->built = true;
+  return 0;
+}
+
+// capture the pipeline into a graph (nothing executes during capture)
+int capture(wlg_batch* b) {
+  WLG_CUDA(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+  int rc = b->prec == WLG_FP64 ? issue<double>(b) : issue<float>(b);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(b->st, &g);
+  if (rc || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    set_error("batch: graph capture failed: %s", cudaGetErrorString(e));
+    cudaGetLastError();
+    return -1;
+  }
+  b->graph = g;
+  WLG_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
+  return 0;
+}
+
+void unbuild(wlg_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->tables) cudaFree(b->tables);
+  b->tables = nullptr;
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->built = false;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wlg_batch_create(int nconf, const int* dims, const int* bcs, const wlg_wloop_parms* parms,
+                     int precision, int device, wlg_batch** out) {
+  set_error("%s", "");
+  if (nconf < 1 || !dims || !bcs || !parms || !out) {
+    set_error("batch_create: bad arguments");
+    return -1;
+  }
+  if (precision != WLG_FP64 && precision != WLG_MIXED) {
+    set_error("batch_create: unknown precision");
+    return -1;
+  }
+  if (wlg_device_count() <= device || device < 0) {
+    set_error("batch_create: no CUDA device %d (no CPU fallback)", device);
+    return -1;
+  }
+  WLG_CUDA(cudaSetDevice(device));
+  wlg_batch* b = new wlg_batch();
+  b->dev = device;
+  b->prec = precision;
+  for (int c = 0; c < nconf; c++) {
+    Cfg f;
+    memset(&f, 0, sizeof(f));
+    for (int i = 0; i < 4; i++)
+      if (dims[4 * c + i] < 2) {
+        set_error("batch_create: lattice %d has an extent < 2", c);
+        delete b;
+        return -1;
+      }
+    f.g = make_geo(dims + 4 * c);
+    f.bc = bcs[c];
+    f.p = parms[c];
+    if ((f.bc != 0 && f.bc != 3) || check_parms(f.g, f.p)) {
+      set_error("batch_create: configuration %d: bad boundary condition or parameters", c);
+      delete b;
+      return -1;
+    }
+    b->cfg.push_back(f);
+  }
+  layout(b);
+  if (plan(b)) {
+    delete b;
+    return -1;
+  }
+  if (ensure_pbuf(b) || cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&b->arena, b->arena_bytes) != cudaSuccess ||
+      cudaMalloc(&b->staging, b->staging_bytes) != cudaSuccess ||
+      cudaMallocHost(&b->wl_host, b->wl_host_doubles * sizeof(double)) != cudaSuccess) {
+    set_error("batch_create: cannot allocate %.2f GB arena: %s", b->arena_bytes / 1e9,
+              cudaGetErrorString(cudaGetLastError()));
+    wlg_batch_destroy(b);
+    return -1;
+  }
+  cudaEventCreate(&b->ev0);
+  cudaEventCreate(&b->ev1);
+  *out = b;
+  return 0;
+}
+
+int wlg_batch_destroy(wlg_batch* b) {
+  if (!b) return 0;
+  cudaSetDevice(b->dev);
+  if (b->st) cudaStreamSynchronize(b->st);
+  unbuild(b);
+  if (b->arena) cudaFree(b->arena);
+  if (b->pbuf) cudaFree(b->pbuf);
+  if (b->tables) cudaFree(b->tables);
+  if (b->staging) cudaFree(b->staging);
+  if (b->wl_host) cudaFreeHost(b->wl_host);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return 0;
+}
+
+int wlg_batch_size(wlg_batch* b) { return b ? (int)b->cfg.size() : 0; }
+
+long long wlg_batch_bytes(wlg_batch* b) { return b ? (long long)b->arena_bytes : 0; }
+
+int wlg_batch_upload(wlg_batch* b, int i, const double* aos) {
+  set_error("%s", "");
+  if (!b || i < 0 || i >= (int)b->cfg.size() || !aos) {
+    set_error("batch_upload: bad arguments");
+    return -1;
+  }
+  WLG_CUDA(cudaSetDevice(b->dev));
+  const Cfg& f = b->cfg[i];
+  size_t bytes = (size_t)4 * 144 * f.g.vol;
+  WLG_CUDA(cudaMemcpyAsync(b->staging, aos, bytes, cudaMemcpyHostToDevice, b->st));
+  if (b->prec == WLG_FP64)
+    aos_to_soa<double>(f.g, (const double*)b->staging, lview<double>(b->arena + f.U, f.D, 4, 0), 0, 4,
+                       b->st);
+  else
+    aos_to_soa<float>(f.g, (const double*)b->staging, lview<float>(b->arena + f.U, f.D, 4, 0), 0, 4,
+                      b->st);
+  WLG_CUDA(cudaStreamSynchronize(b->st));
+  return get_error()[0] ? -1 : 0;
+}
+
+int wlg_batch_generate(wlg_batch* b, const uint64_t* seeds, const double* eps) {
+  set_error("%s", "");
+  if (!b || !seeds || !eps) {
+    set_error("batch_generate: bad arguments");
+    return -1;
+  }
+  WLG_CUDA(cudaSetDevice(b->dev));
+  for (size_t c = 0; c < b->cfg.size(); c++) {
+    const Cfg& f = b->cfg[c];
+    if (b->prec == WLG_FP64)
+      generate_soa<double>(f.g, f.bc, seeds[c], eps[c], lview<double>(b->arena + f.U, f.D, 4, 0),
+                           b->st);
+    else
+      generate_soa<float>(f.g, f.bc, seeds[c], eps[c], lview<float>(b->arena + f.U, f.D, 4, 0),
+                          b->st);
+  }
+  WLG_CUDA(cudaStreamSynchronize(b->st));
+  return get_error()[0] ? -1 : 0;
+}
+
+int wlg_batch_snapshot(wlg_batch* b) {
+  set_error("%s", "");
+  WLG_CUDA(cudaSetDevice(b->dev));
+  for (const Cfg& f : b->cfg)
+    WLG_CUDA(cudaMemcpyAsync(b->arena + f.U0, b->arena + f.U, 4 * f.D * elem_bytes(b),
+                             cudaMemcpyDeviceToDevice, b->st));
+  WLG_CUDA(cudaStreamSynchronize(b->st));
+  return 0;
+}
+
+int wlg_batch_restore(wlg_batch* b) {
+  set_error("%s", "");
+  WLG_CUDA(cudaSetDevice(b->dev));
+  for (const Cfg& f : b->cfg)
+    WLG_CUDA(cudaMemcpyAsync(b->arena + f.U, b->arena + f.U0, 4 * f.D * elem_bytes(b),
+                             cudaMemcpyDeviceToDevice, b->st));
+  return 0;
+}
+
+int wlg_batch_run(wlg_batch* b) {
+  set_error("%s", "");
+  if (!b) {
+    set_error("batch_run: null batch");
+    return -1;
+  }
+  WLG_CUDA(cudaSetDevice(b->dev));
+  if (build(b)) return -1;
+  WLG_CUDA(cudaEventRecord(b->ev0, b->st));
+  if (b->exec) {
+    WLG_CUDA(cudaGraphLaunch(b->exec, b->st));
+  } else {
+    int rc = b->prec == WLG_FP64 ? issue<double>(b) : issue<float>(b);
+    if (rc) return -1;
+  }
+  WLG_CUDA(cudaEventRecord(b->ev1, b->st));
+  WLG_CUDA(cudaStreamSynchronize(b->st));
+  cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("batch_run: %s", cudaGetErrorString(e));
+    return -1;
+  }
+  // the first run executed the kernels directly; later runs replay a graph
+  if (b->use_graph && !b->exec && capture(b)) return -1;
+  return 0;
+}
+
+int wlg_batch_use_graph(wlg_batch* b, int on) {
+  if (!b) return -1;
+  b->use_graph = on != 0;
+  return 0;
+}
+
+// device bytes a batch of these configurations would hold (no allocation)
+long long wlg_batch_estimate_bytes(int nconf, const int* dims, const int* bcs,
+                                   const wlg_wloop_parms* parms, int precision) {
+  if (nconf < 1 || !dims || !bcs || !parms) return -1;
+  wlg_batch tmp;
+  tmp.prec = precision;
+  for (int c = 0; c < nconf; c++) {
+    Cfg f;
+    memset(&f, 0, sizeof(f));
+    f.g = make_geo(dims + 4 * c);
+    f.bc = bcs[c];
+    f.p = parms[c];
+    if (check_parms(f.g, f.p)) return -1;
+    tmp.cfg.push_back(f);
+  }
+  layout(&tmp);
+  if (plan(&tmp)) return -1;
+  return (long long)(tmp.arena_bytes + tmp.pbuf_bytes + tmp.staging_bytes + (1 << 20));
+}
+
+int wlg_batch_result(wlg_batch* b, int i, double* wl_mat) {
+  set_error("%s", "");
+  if (!b || i < 0 || i >= (int)b->cfg.size() || !wl_mat) {
+    set_error("batch_result: bad arguments");
+    return -1;
+  }
+  const Cfg& f = b->cfg[i];
+  memcpy(wl_mat, b->wl_host + f.wl_host, f.nwl * sizeof(double));
+  return 0;
+}
+
+int wlg_batch_stats(wlg_batch* b, double* last_ms, int* kernels_per_run) {
+  if (!b) return -1;
+  if (last_ms) *last_ms = b->last_ms;
+  if (kernels_per_run) *kernels_per_run = b->kernels;
+  return 0;
+}
+
+void* wlg_batch_stream(wlg_batch* b) { return b ? (void*)b->st : nullptr; }
+
+int wlg_batch_set_contract_shape(wlg_batch* b, int G, int SB, int nCB, int block) {
+  set_error("%s", "");
+  if (!b || G < 0 || G > 4 || SB < 0 || SB > 2 || nCB < 0 ||
+      (block != 0 && (block % 32 != 0 || block > 128))) {
+    set_error("batch_set_contract_shape: bad shape");
+    return -1;
+  }
+  WLG_CUDA(cudaSetDevice(b->dev));
+  WLG_CUDA(cudaStreamSynchronize(b->st));
+  b->tG = G;
+  b->tSB = SB;
+  b->tNCB = nCB;
+  b->tBlock = block;
+  unbuild(b);
+  if (plan(b) || ensure_pbuf(b)) return -1;
+  return 0;
+}
+
+}  // extern "C"

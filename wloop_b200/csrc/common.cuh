@@ -82,6 +82,58 @@ template <class T> struct Links {
   typename V2<T>::t* p[4];
 };
 
+// largest c in [0,n) with pre[c] <= w: the lattice that owns flattened work
+// item w of a batched launch (pre is the prefix of per-lattice work)
+__device__ __forceinline__ int find_item(const long long* __restrict__ pre, int n, long long w) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(pre + mid) <= w)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Arguments of one smearing launch on one lattice (see the item functions of
+// smear.cu); the batched kernels take an array of these.
+template <class T> struct SArgs {
+  Geo g;
+  Links<T> U;               // links read (staples / linear combination)
+  Links<T> D;               // links written (APE destination, spatial-HYP level 2)
+  typename V2<T>::t* aux0;  // HYP first-level / spatial-HYP level-1 scratch
+  typename V2<T>::t* aux1;  // HYP second-level scratch
+  double a, b;              // linear combination a U + b S (APE: a = alpha)
+  int proj, iter, mu0, nmu, bc;
+};
+
+// Arguments of one spatial-line step (loops.cu): dst = src(x) level(x+(R-1)k)
+template <class T> struct LArgs {
+  Geo g;
+  int msl, R;
+  const typename V2<T>::t* level;
+  const typename V2<T>::t* src;
+  typename V2<T>::t* dst;
+};
+
+// Arguments of one contraction launch on one lattice (loops.cu)
+template <class T> struct CArgs {
+  Geo g;
+  const typename V2<T>::t* u0;     // temporal links
+  const typename V2<T>::t* lines;  // [msl][3] spatial lines of length R
+  int msl, mwlt, R, ngrp, nCB;
+  double* partial;
+};
+
+// Arguments of one partial-sum reduction (loops.cu): wl for spatial extent r
+struct RArgs {
+  int msl, mwlt, mwlr, r, G, ngrp, nCB, nout;
+  double norm;
+  const double* partial;
+  double* wl;
+};
+
 // elements (of V2<T>::t) per 32-site tile and per direction array
 template <class T> struct Tile;
 template <> struct Tile<double> { enum { TS = 288 }; };  // 9 x 32 double2

@@ -83,6 +83,25 @@ void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
 void contract_reduce(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mwlr, int r,
                      const double* partial, double* wl_mat, cudaStream_t st);
 
+// ---- batched stages (one launch over many lattices) ------------------------
+// A: device array of n per-lattice argument records; pre: device array of
+// n+1 prefix sums of the per-lattice work items (blocks for the contraction).
+template <class T>
+void smear_batch(int stage, const SArgs<T>* A, const long long* pre, int n, long long total,
+                 cudaStream_t st);
+enum { BATCH_HYP3 = 0, BATCH_HYP2, BATCH_HYP1, BATCH_APE, BATCH_HYP3D1, BATCH_HYP3D2 };
+template <class T>
+void line_step_batch(const LArgs<T>* A, const long long* pre, int n, long long total,
+                     cudaStream_t st);
+template <class T>
+void contract_batch(int G, int SB, const CArgs<T>* A, const long long* pre, int n, long long nblocks,
+                    int block, size_t smem, cudaStream_t st);
+template <class T> size_t contract3_smem(const ContractPlan& p, int msl);
+RArgs reduce_args(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mwlr, int r,
+                  const double* partial, double* wl_mat);
+void contract_reduce_batch(const RArgs* A, const long long* pre, int n, long long total,
+                           cudaStream_t st);
+
 // ---- layout (layout.cu) ---------------------------------------------------
 // AoS lexicographic FP64 [V][4][18] <-> SoA field of type T (directions [mu0,mu1)).
 template <class T>

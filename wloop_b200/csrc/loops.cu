@@ -11,7 +11,8 @@
 // owns one column (xs,k) at one start slice x0 and G bottom levels; the
 // msl*G traces of each T are summed over the warp by a transposing shuffle
 // reduction and accumulated in a per-warp shared-memory row, so no atomics
-// and a fixed summation order.
+// and a fixed summation order.  Every stage also has a batched kernel that
+// covers many lattices in one launch (flattened work list, find_item).
 #include "internal.h"
 
 namespace wlg {
@@ -19,25 +20,38 @@ namespace wlg {
 // lines_dst[sl][k](x) = lines_src[sl][k](x) * level[sl][k](x + (R-1) k)
 // (compute_uk_long, wloop.c:207-258, multiplied from the other end so the
 // update is in place).
-template <class T>
-__global__ void __launch_bounds__(128) k_line_step(Geo g, int msl, int R,
-                                                   const typename V2<T>::t* level,
-                                                   const typename V2<T>::t* src,
-                                                   typename V2<T>::t* dst) {
-  const long long n = (long long)msl * 3 * g.vol;
+// w in [0, msl*3*V)
+template <class T> __device__ __forceinline__ void line_step_item(const LArgs<T>& A, long long w) {
+  const Geo& g = A.g;
+  int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+  int k = q % 3;
+  int x[4];
+  coords(g, s, x);
+  int y = shift(g, s, x[k + 1], k + 1, (A.R - 1) % g.n[k + 1]);
+  M3<T> a, b, c;
+  const size_t off = (size_t)q * link_elems<T>(g.vol);
+  ld(a, A.src + off, g.vol, s);
+  ld(b, A.level + off, g.vol, y);
+  mul(c, a, b);
+  st(A.dst + off, g.vol, s, c);
+}
+
+template <class T> __global__ void __launch_bounds__(128) k_line_step(LArgs<T> A) {
+  const long long n = (long long)A.msl * 3 * A.g.vol;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
+       w += (long long)gridDim.x * blockDim.x)
+    line_step_item<T>(A, w);
+}
+
+// batched: pre[c] = first work item of lattice c
+template <class T>
+__global__ void __launch_bounds__(128) kb_line_step(const LArgs<T>* __restrict__ A,
+                                                    const long long* __restrict__ pre, int n,
+                                                    long long total) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total;
        w += (long long)gridDim.x * blockDim.x) {
-    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
-    int k = q % 3;
-    int x[4];
-    coords(g, s, x);
-    int y = shift(g, s, x[k + 1], k + 1, (R - 1) % g.n[k + 1]);
-    M3<T> a, b, c;
-    const size_t off = (size_t)q * link_elems<T>(g.vol);
-    ld(a, src + off, g.vol, s);
-    ld(b, level + off, g.vol, y);
-    mul(c, a, b);
-    st(dst + off, g.vol, s, c);
+    const int c = find_item(pre, n, w);
+    line_step_item<T>(A[c], w - pre[c]);
   }
 }
 
@@ -47,7 +61,14 @@ void line_step(const Geo& g, int msl, int R, const typename V2<T>::t* level,
   long long n = (long long)msl * 3 * g.vol;
   long long grid = (n + 127) / 128;
   if (grid > num_sms() * 32) grid = num_sms() * 32;
-  k_line_step<T><<<(int)grid, 128, 0, st>>>(g, msl, R, level, src, dst);
+  LArgs<T> A;
+  A.g = g;
+  A.msl = msl;
+  A.R = R;
+  A.level = level;
+  A.src = src;
+  A.dst = const_cast<typename V2<T>::t*>(dst);
+  k_line_step<T><<<(int)grid, 128, 0, st>>>(A);
   WLG_LAUNCH_CHECK("line_step");
 }
 
@@ -88,114 +109,10 @@ __device__ __forceinline__ double wt_reduce(double (&v)[KP], int lane) {
 template <int K> struct Pow2 { enum { v = (K <= 1) ? 1 : (K <= 2) ? 2 : (K <= 4) ? 4 : (K <= 8) ? 8 : (K <= 16) ? 16 : 32 }; };
 
 // ---------------------------------------------------------------------------
-// contraction kernel
-//   grid.x = N0 * ngrp * nCB   (x0 fastest: concurrent blocks share columns)
-//   partial[((x0*ngrp + grp)*nCB + cb)][T][g][s2]
-// ---------------------------------------------------------------------------
-template <class T, int G, int SB>
-__global__ void __launch_bounds__(128) k_contract(Geo g, const typename V2<T>::t* __restrict__ u0,
-                                                  const typename V2<T>::t* __restrict__ lines,
-                                                  int msl, int mwlt, int R, int ngrp, int nCB,
-                                                  double* __restrict__ partial) {
-  extern __shared__ double acc[];  // [nwarps][mwlt][G][msl]
-  constexpr int K = G * SB;
-  constexpr int KP = Pow2<K>::v;
-  static_assert(K <= 32, "G*SB must not exceed 32");
-
-  const int N0 = g.n[0], vs = g.vs, vol = g.vol;
-  int b = blockIdx.x;
-  const int x0 = b % N0;
-  b /= N0;
-  const int grp = b % ngrp;
-  const int cb = b / ngrp;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int rowlen = mwlt * G * msl;
-  double* wacc = acc + (size_t)warp * rowlen;
-  for (int i = lane; i < rowlen; i += 32) wacc[i] = 0.0;
-  __syncwarp();
-
-  const int s1_0 = grp * G;
-  const int ncol = 3 * vs;
-  const int per = (ncol + nCB - 1) / nCB;
-  const int c_begin = cb * per;
-  const int c_end = min(ncol, c_begin + per);
-  const size_t fstride = link_elems<T>(vol);
-
-  // all lanes of a warp iterate together so shuffles stay converged
-  for (int cbase = c_begin; cbase < c_end; cbase += blockDim.x) {
-    const int col = cbase + threadIdx.x;
-    const bool active = col < c_end;
-    const int cc = active ? col : c_begin;
-    const int k = cc / vs, xs = cc - k * vs;
-    // xs + R k (coordinates inside the time slice)
-    int x1 = xs / g.st[1], r = xs - x1 * g.st[1];
-    int x2 = r / g.st[2], x3 = r - x2 * g.st[2];
-    int xsR;
-    {
-      int xx[3] = {x1, x2, x3};
-      int y = xx[k] + (R % g.n[k + 1]);
-      if (y >= g.n[k + 1]) y -= g.n[k + 1];
-      xx[k] = y;
-      xsR = xx[0] * g.st[1] + xx[1] * g.st[2] + xx[2];
-    }
-    M3<T> C[G];
-#pragma unroll
-    for (int gi = 0; gi < G; gi++) {
-      int s1 = min(s1_0 + gi, msl - 1);
-      ld(C[gi], lines + ((size_t)s1 * 3 + k) * fstride, vol, x0 * vs + xs);
-    }
-    int t0 = x0;
-    for (int tt = 1; tt <= mwlt; tt++) {
-      M3<T> u, tmp;
-      ld(u, u0, vol, t0 * vs + xs);
-#pragma unroll
-      for (int gi = 0; gi < G; gi++) {
-        mul_da(tmp, u, C[gi]);
-        C[gi] = tmp;
-      }
-      ld(u, u0, vol, t0 * vs + xsR);
-#pragma unroll
-      for (int gi = 0; gi < G; gi++) {
-        mul(tmp, C[gi], u);
-        C[gi] = tmp;
-      }
-      t0 = (t0 + 1 == N0) ? 0 : t0 + 1;  // = x0+T mod N0, the top slice
-      const int stop = t0 * vs + xs;
-      for (int sb = 0; sb < msl; sb += SB) {
-        double v[KP];
-#pragma unroll
-        for (int i = 0; i < KP; i++) v[i] = 0.0;
-#pragma unroll
-        for (int j = 0; j < SB; j++) {
-          const int s2 = sb + j;
-          if (s2 < msl) {
-            M3<T> l;
-            ld(l, lines + ((size_t)s2 * 3 + k) * fstride, vol, stop);
-#pragma unroll
-            for (int gi = 0; gi < G; gi++) v[gi * SB + j] = active ? (double)retr_dag(l, C[gi]) : 0.0;
-          }
-        }
-        double sum = wt_reduce<KP>(v, lane);
-        const int idx = lane >> (5 - Log2<KP>::v);
-        if ((lane & ((32 / KP) - 1)) == 0 && idx < K) {
-          const int gi = idx / SB, s2 = sb + idx % SB;
-          if (s2 < msl) wacc[((tt - 1) * G + gi) * msl + s2] += sum;
-        }
-      }
-    }
-  }
-  __syncthreads();
-  // partial layout [x0][grp][cb] (read back by k_contract_reduce)
-  double* out = partial + ((size_t)(x0 * ngrp + grp) * nCB + cb) * rowlen;
-  for (int i = threadIdx.x; i < rowlen; i += blockDim.x) {
-    double s = 0.0;
-    for (int w = 0; w < nwarps; w++) s += acc[(size_t)w * rowlen + i];
-    out[i] = s;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// contraction kernel, second form: same work split as k_contract, with
+// contraction kernel, second form.  One thread owns one column (xs,k) at
+// one start slice x0 and G bottom levels; grid.x = N0 * ngrp * nCB with x0
+// fastest (concurrent blocks share columns through L2); the block writes
+// partial[((x0*ngrp + grp)*nCB + cb)][T][g][s2].  Per T-step:
 //  * C updated in place (6 temporaries per product instead of a full matrix),
 //  * the next T-step's temporal links loaded right after they are consumed,
 //    so their latency overlaps the traces and the reduction,
@@ -346,8 +263,11 @@ static void launch_contract2(const Geo& g, const ContractPlan& p, const typename
                              double* partial, cudaStream_t st) {
   constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
   auto kern = k_contract2<T, G, SB, MINB>;
-  if (p.smem > 48 * 1024)
+  static size_t smem_set = 48 * 1024;
+  if (p.smem > smem_set) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    smem_set = p.smem;
+  }
   int grid = g.n[0] * p.ngrp * p.nCB;
   kern<<<grid, p.block, p.smem, st>>>(g, u0, lines, msl, mwlt, R, p.ngrp, p.nCB, partial);
   WLG_LAUNCH_CHECK("contract");
@@ -361,19 +281,6 @@ static void launch_contract2_sb(const Geo& g, const ContractPlan& p, const typen
     launch_contract2<T, G, 2>(g, p, u0, lines, msl, mwlt, R, partial, st);
   else
     launch_contract2<T, G, 1>(g, p, u0, lines, msl, mwlt, R, partial, st);
-}
-
-template <class T, int G>
-static void launch_contract_G(const Geo& g, const ContractPlan& p,
-                              const typename V2<T>::t* u0, const typename V2<T>::t* lines,
-                              int msl, int mwlt, int R, double* partial, cudaStream_t st) {
-  constexpr int SB = (32 / G) < 8 ? (32 / G) : 8;
-  auto kern = k_contract<T, G, SB>;
-  if (p.smem > 48 * 1024)
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
-  int grid = g.n[0] * p.ngrp * p.nCB;
-  kern<<<grid, p.block, p.smem, st>>>(g, u0, lines, msl, mwlt, R, p.ngrp, p.nCB, partial);
-  WLG_LAUNCH_CHECK("contract");
 }
 
 // ---------------------------------------------------------------------------
@@ -419,20 +326,21 @@ template <> __device__ __forceinline__ void ld_stage<float>(M3<float>& m, const 
   }
 }
 
-template <class T, int G, int SB, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_contract3(Geo g,
-                                                         const typename V2<T>::t* __restrict__ u0,
-                                                         const typename V2<T>::t* __restrict__ lines,
-                                                         int msl, int mwlt, int R, int ngrp,
-                                                         int nCB, double* __restrict__ partial) {
+template <class T, int G, int SB>
+__device__ __forceinline__ void contract3_body(const CArgs<T>& A, int bid) {
   extern __shared__ double acc[];  // [nwarps][mwlt][G][msl] doubles, then the line stage
   constexpr int K = G * SB;
   constexpr int KP = Pow2<K>::v;
   constexpr int NQ = Chunks<T>::N;
   static_assert(K <= 32, "G*SB must not exceed 32");
 
+  const Geo& g = A.g;
+  const typename V2<T>::t* __restrict__ u0 = A.u0;
+  const typename V2<T>::t* __restrict__ lines = A.lines;
+  const int msl = A.msl, mwlt = A.mwlt, R = A.R, ngrp = A.ngrp, nCB = A.nCB;
+  double* __restrict__ partial = A.partial;
   const int N0 = g.n[0], vs = g.vs, vol = g.vol;
-  int b = blockIdx.x;
+  int b = bid;
   const int x0 = b % N0;
   b /= N0;
   const int grp = b % ngrp;
@@ -536,17 +444,47 @@ __global__ void __launch_bounds__(128, MINB) k_contract3(Geo g,
   }
 }
 
+template <class T> size_t contract3_smem(const ContractPlan& p, int msl) {
+  return p.smem + (size_t)msl * Chunks<T>::N * p.block * 16;
+}
+
+template <class T, int G, int SB, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_contract3(CArgs<T> A) {
+  contract3_body<T, G, SB>(A, blockIdx.x);
+}
+
+// batched: the blocks of all lattices in one grid; pre[c] = first block of lattice c
+template <class T, int G, int SB, int MINB>
+__global__ void __launch_bounds__(128, MINB) kb_contract3(const CArgs<T>* __restrict__ A,
+                                                          const long long* __restrict__ pre, int n) {
+  const int c = find_item(pre, n, (long long)blockIdx.x);
+  contract3_body<T, G, SB>(A[c], (int)(blockIdx.x - pre[c]));
+}
+
 template <class T, int G, int SB>
 static void launch_contract3(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
                              const typename V2<T>::t* lines, int msl, int mwlt, int R,
                              double* partial, cudaStream_t st) {
   constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
   auto kern = k_contract3<T, G, SB, MINB>;
-  size_t smem = p.smem + (size_t)msl * Chunks<T>::N * p.block * 16;
-  if (smem > 48 * 1024)
+  size_t smem = contract3_smem<T>(p, msl);
+  static size_t smem_set = 48 * 1024;  // attribute is raised only when needed (never under capture)
+  if (smem > smem_set) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_set = smem;
+  }
   int grid = g.n[0] * p.ngrp * p.nCB;
-  kern<<<grid, p.block, smem, st>>>(g, u0, lines, msl, mwlt, R, p.ngrp, p.nCB, partial);
+  CArgs<T> A;
+  A.g = g;
+  A.u0 = u0;
+  A.lines = lines;
+  A.msl = msl;
+  A.mwlt = mwlt;
+  A.R = R;
+  A.ngrp = p.ngrp;
+  A.nCB = p.nCB;
+  A.partial = partial;
+  kern<<<grid, p.block, smem, st>>>(A);
   WLG_LAUNCH_CHECK("contract");
 }
 
@@ -564,16 +502,6 @@ template <class T>
 void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
               const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
               cudaStream_t st) {
-  if (p.variant == 1) {
-    switch (p.G) {
-      case 1: launch_contract_G<T, 1>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
-      case 2: launch_contract_G<T, 2>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
-      case 3: launch_contract_G<T, 3>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
-      case 4: launch_contract_G<T, 4>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
-      case 6: launch_contract_G<T, 6>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
-      default: set_error("contract: unsupported G=%d", p.G); return;
-    }
-  }
   if (p.variant == 3) {
     switch (p.G) {
       case 1: launch_contract3_sb<T, 1>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
@@ -594,32 +522,116 @@ void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
 }
 
 // wl_mat[sl1 + msl*(sl2 + msl*(t + mwlt*(r + mwlr*x0)))] (wloop_parms.c:431-434)
-__global__ void k_contract_reduce(int N0, int msl, int mwlt, int mwlr, int r, int G, int ngrp,
-                                  int nCB, double norm, const double* __restrict__ partial,
-                                  double* __restrict__ wl) {
-  const int nout = N0 * mwlt * msl * msl;
-  const int rowlen = mwlt * G * msl;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nout; i += gridDim.x * blockDim.x) {
-    int s1 = i % msl, q = i / msl;
-    int s2 = q % msl;
-    q /= msl;
-    int t = q % mwlt, x0 = q / mwlt;
-    int grp = s1 / G, gi = s1 - grp * G;
-    const double* p = partial + (size_t)((x0 * ngrp + grp) * nCB) * rowlen + (t * G + gi) * msl + s2;
-    double s = 0.0;
-    for (int cb = 0; cb < nCB; cb++) s += p[(size_t)cb * rowlen];
-    wl[s1 + msl * (s2 + msl * (t + mwlt * (r + mwlr * x0)))] = s / norm;
+__device__ __forceinline__ void reduce_item(const RArgs& A, int i) {
+  const int msl = A.msl, mwlt = A.mwlt;
+  const int rowlen = mwlt * A.G * msl;
+  int s1 = i % msl, q = i / msl;
+  int s2 = q % msl;
+  q /= msl;
+  int t = q % mwlt, x0 = q / mwlt;
+  int grp = s1 / A.G, gi = s1 - grp * A.G;
+  const double* p =
+      A.partial + (size_t)((x0 * A.ngrp + grp) * A.nCB) * rowlen + (t * A.G + gi) * msl + s2;
+  double s = 0.0;
+  for (int cb = 0; cb < A.nCB; cb++) s += p[(size_t)cb * rowlen];
+  A.wl[s1 + msl * (s2 + msl * (t + mwlt * (A.r + A.mwlr * x0)))] = s / A.norm;
+}
+
+__global__ void k_contract_reduce(RArgs A, int nout) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nout; i += gridDim.x * blockDim.x)
+    reduce_item(A, i);
+}
+
+__global__ void kb_contract_reduce(const RArgs* __restrict__ A, const long long* __restrict__ pre,
+                                   int n, long long total) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total;
+       w += (long long)gridDim.x * blockDim.x) {
+    const int c = find_item(pre, n, w);
+    reduce_item(A[c], (int)(w - pre[c]));
   }
+}
+
+RArgs reduce_args(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mwlr, int r,
+                  const double* partial, double* wl_mat) {
+  RArgs A;
+  A.msl = msl;
+  A.mwlt = mwlt;
+  A.mwlr = mwlr;
+  A.r = r;
+  A.G = p.G;
+  A.ngrp = p.ngrp;
+  A.nCB = p.nCB;
+  A.norm = 9.0 * (double)g.n[1] * (double)g.n[2] * (double)g.n[3];  // wloop.c:535
+  A.partial = partial;
+  A.wl = wl_mat;
+  A.nout = g.n[0] * mwlt * msl * msl;
+  return A;
 }
 
 void contract_reduce(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mwlr, int r,
                      const double* partial, double* wl_mat, cudaStream_t st) {
-  int nout = g.n[0] * mwlt * msl * msl;
-  int grid = (nout + 255) / 256;
-  double norm = 9.0 * (double)g.n[1] * (double)g.n[2] * (double)g.n[3];  // wloop.c:535
-  k_contract_reduce<<<grid, 256, 0, st>>>(g.n[0], msl, mwlt, mwlr, r, p.G, p.ngrp, p.nCB,
-                                          norm, partial, wl_mat);
+  RArgs A = reduce_args(g, p, msl, mwlt, mwlr, r, partial, wl_mat);
+  int grid = (A.nout + 255) / 256;
+  k_contract_reduce<<<grid, 256, 0, st>>>(A, A.nout);
   WLG_LAUNCH_CHECK("contract_reduce");
+}
+
+// ---- batched launchers ----------------------------------------------------
+static int bgrid(long long total, int block) {
+  long long gsz = (total + block - 1) / block;
+  long long cap = (long long)num_sms() * 32;
+  return (int)(gsz < 1 ? 1 : (gsz > cap ? cap : gsz));
+}
+
+template <class T>
+void line_step_batch(const LArgs<T>* A, const long long* pre, int n, long long total,
+                     cudaStream_t st) {
+  if (n <= 0 || total <= 0) return;
+  kb_line_step<T><<<bgrid(total, 128), 128, 0, st>>>(A, pre, n, total);
+  WLG_LAUNCH_CHECK("line_step_batch");
+}
+
+void contract_reduce_batch(const RArgs* A, const long long* pre, int n, long long total,
+                           cudaStream_t st) {
+  if (n <= 0 || total <= 0) return;
+  kb_contract_reduce<<<bgrid(total, 256), 256, 0, st>>>(A, pre, n, total);
+  WLG_LAUNCH_CHECK("contract_reduce_batch");
+}
+
+template <class T, int G, int SB>
+static void launch_contract3_batch(const CArgs<T>* A, const long long* pre, int n,
+                                   long long nblocks, int block, size_t smem, cudaStream_t st) {
+  constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
+  auto kern = kb_contract3<T, G, SB, MINB>;
+  static size_t smem_set = 48 * 1024;  // raised only when needed (never under capture)
+  if (smem > smem_set) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_set = smem;
+  }
+  kern<<<(unsigned)nblocks, block, smem, st>>>(A, pre, n);
+  WLG_LAUNCH_CHECK("contract_batch");
+}
+
+template <class T>
+void contract_batch(int G, int SB, const CArgs<T>* A, const long long* pre, int n, long long nblocks,
+                    int block, size_t smem, cudaStream_t st) {
+  if (n <= 0 || nblocks <= 0) return;
+  if (SB == 2) {
+    switch (G) {
+      case 1: launch_contract3_batch<T, 1, 2>(A, pre, n, nblocks, block, smem, st); return;
+      case 2: launch_contract3_batch<T, 2, 2>(A, pre, n, nblocks, block, smem, st); return;
+      case 3: launch_contract3_batch<T, 3, 2>(A, pre, n, nblocks, block, smem, st); return;
+      case 4: launch_contract3_batch<T, 4, 2>(A, pre, n, nblocks, block, smem, st); return;
+    }
+  } else {
+    switch (G) {
+      case 1: launch_contract3_batch<T, 1, 1>(A, pre, n, nblocks, block, smem, st); return;
+      case 2: launch_contract3_batch<T, 2, 1>(A, pre, n, nblocks, block, smem, st); return;
+      case 3: launch_contract3_batch<T, 3, 1>(A, pre, n, nblocks, block, smem, st); return;
+      case 4: launch_contract3_batch<T, 4, 1>(A, pre, n, nblocks, block, smem, st); return;
+    }
+  }
+  set_error("contract_batch: unsupported G=%d SB=%d", G, SB);
 }
 
 template void line_step<double>(const Geo&, int, int, const double2*, const double2*, double2*,
@@ -631,4 +643,17 @@ template void contract<double>(const Geo&, const ContractPlan&, const double2*, 
 template void contract<float>(const Geo&, const ContractPlan&, const float2*, const float2*, int,
                               int, int, double*, cudaStream_t);
 
+}  // namespace wlg
+
+namespace wlg {
+template void line_step_batch<double>(const LArgs<double>*, const long long*, int, long long,
+                                      cudaStream_t);
+template void line_step_batch<float>(const LArgs<float>*, const long long*, int, long long,
+                                     cudaStream_t);
+template void contract_batch<double>(int, int, const CArgs<double>*, const long long*, int,
+                                     long long, int, size_t, cudaStream_t);
+template void contract_batch<float>(int, int, const CArgs<float>*, const long long*, int, long long,
+                                    int, size_t, cudaStream_t);
+template size_t contract3_smem<double>(const ContractPlan&, int);
+template size_t contract3_smem<float>(const ContractPlan&, int);
 }  // namespace wlg

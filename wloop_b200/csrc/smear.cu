@@ -8,6 +8,8 @@
 // input field roughly once per kernel.  Staple products run in T (FP64, or
 // FP32 in the mixed form); the linear combination and the SU(3) projection
 // always run in FP64.
+#include <string.h>
+
 #include "internal.h"
 
 namespace wlg {
@@ -55,189 +57,191 @@ __device__ __forceinline__ void lcomb_project(M3<double>& v, double a, const M3<
 }
 
 // ---------------------------------------------------------------------------
-// HYP level with alpha3 (decorated_links1, hyp_links.c:320-373):
-//   vbar[p(mu,eta)](x,mu) = P[(1-a3) U + a3/2 * S_eta(U)]
+// Item functions: one output link each, w = local work index of one lattice
+// (site fastest).  The single-lattice kernels below and the batched kernels
+// of batch.cu (flattened work lists over many lattices) both call them.
 // ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(128) k_hyp_l3(Geo g, Links<T> U, typename V2<T>::t* vbar,
-                                                double a, double b, int proj, int iter) {
-  const long long n = 12LL * g.vol;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
-       w += (long long)gridDim.x * blockDim.x) {
-    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
-    int mu = q / 3, eta = (mu + 1 + q % 3) & 3;
-    int x[4];
-    coords(g, s, x);
-    M3<T> S, u;
-    zero(S);
-    add_staples(S, g, x, s, U.p[eta], U.p[mu], mu, eta);
-    ld(u, U.p[mu], g.vol, s);
-    M3<double> v;
-    lcomb_project(v, a, u, b, S, proj, iter);
-    M3<T> o;
-    cvt(o, v);
-    st(fld<T>(vbar, g.vol, hyp_pair(mu, eta), mu, 4), g.vol, s, o);
-  }
+
+// HYP level with alpha3 (decorated_links1, hyp_links.c:320-373):
+//   vbar[p(mu,eta)](x,mu) = P[(1-a3) U + a3/2 * S_eta(U)];  w in [0, 12V)
+template <class T> __device__ __forceinline__ void hyp_l3_item(const SArgs<T>& A, long long w) {
+  const Geo& g = A.g;
+  int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+  int mu = q / 3, eta = (mu + 1 + q % 3) & 3;
+  int x[4];
+  coords(g, s, x);
+  M3<T> S, u;
+  zero(S);
+  add_staples(S, g, x, s, A.U.p[eta], A.U.p[mu], mu, eta);
+  ld(u, A.U.p[mu], g.vol, s);
+  M3<double> v;
+  lcomb_project(v, A.a, u, A.b, S, A.proj, A.iter);
+  M3<T> o;
+  cvt(o, v);
+  st(fld<T>(A.aux0, g.vol, hyp_pair(mu, eta), mu, 4), g.vol, s, o);
 }
 
-// ---------------------------------------------------------------------------
 // HYP level with alpha2 (decorated_links2, hyp_links.c:244-317):
 //   vtil[p(mu,nu)](x,mu) = P[(1-a2) U + a2/4 * sum_{rho != mu,nu} S_rho]
-//   rho-links from vbar[p(mu,nu)], mu-links from vbar[p(nu,rho)]
-// ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(128) k_hyp_l2(Geo g, Links<T> U, const typename V2<T>::t* vbar,
-                                                typename V2<T>::t* vtil, double a, double b,
-                                                int proj, int iter) {
-  const long long n = 12LL * g.vol;
-  typename V2<T>::t* vb = const_cast<typename V2<T>::t*>(vbar);
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
-       w += (long long)gridDim.x * blockDim.x) {
-    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
-    int mu = q / 3, nu = (mu + 1 + q % 3) & 3;
-    int x[4];
-    coords(g, s, x);
-    int pmn = hyp_pair(mu, nu);
-    M3<T> S, u;
-    zero(S);
+//   rho-links from vbar[p(mu,nu)], mu-links from vbar[p(nu,rho)];  w in [0, 12V)
+template <class T> __device__ __forceinline__ void hyp_l2_item(const SArgs<T>& A, long long w) {
+  const Geo& g = A.g;
+  int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+  int mu = q / 3, nu = (mu + 1 + q % 3) & 3;
+  int x[4];
+  coords(g, s, x);
+  int pmn = hyp_pair(mu, nu);
+  M3<T> S, u;
+  zero(S);
 #pragma unroll
-    for (int rho = 0; rho < 4; rho++) {
-      if (rho == mu || rho == nu) continue;
-      add_staples(S, g, x, s, fld<T>(vb, g.vol, pmn, rho, 4),
-                  fld<T>(vb, g.vol, hyp_pair(nu, rho), mu, 4), mu, rho);
-    }
-    ld(u, U.p[mu], g.vol, s);
-    M3<double> v;
-    lcomb_project(v, a, u, b, S, proj, iter);
-    M3<T> o;
-    cvt(o, v);
-    st(fld<T>(vtil, g.vol, pmn, mu, 4), g.vol, s, o);
+  for (int rho = 0; rho < 4; rho++) {
+    if (rho == mu || rho == nu) continue;
+    add_staples(S, g, x, s, fld<T>(A.aux0, g.vol, pmn, rho, 4),
+                fld<T>(A.aux0, g.vol, hyp_pair(nu, rho), mu, 4), mu, rho);
   }
+  ld(u, A.U.p[mu], g.vol, s);
+  M3<double> v;
+  lcomb_project(v, A.a, u, A.b, S, A.proj, A.iter);
+  M3<T> o;
+  cvt(o, v);
+  st(fld<T>(A.aux1, g.vol, pmn, mu, 4), g.vol, s, o);
 }
 
-// ---------------------------------------------------------------------------
 // HYP level with alpha1 (decorated_links3, hyp_links.c:194-241) and the copy
-// back into the gauge field (:432-447).  U is written in place: each thread
-// reads only its own U(x,mu) for the linear combination.
-// ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(128) k_hyp_l1(Geo g, Links<T> U, const typename V2<T>::t* vtil,
-                                                double a, double b, int proj, int iter, int mu0,
-                                                int nmu, int bc) {
-  const long long n = (long long)nmu * g.vol;
-  typename V2<T>::t* vt = const_cast<typename V2<T>::t*>(vtil);
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
-       w += (long long)gridDim.x * blockDim.x) {
-    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
-    int mu = mu0 + q;
-    int x[4];
-    coords(g, s, x);
-    M3<T> S, u;
-    zero(S);
+// back into the gauge field (:432-447), in place: each item reads only its
+// own U(x,mu) for the linear combination.  w in [0, nmu V)
+template <class T> __device__ __forceinline__ void hyp_l1_item(const SArgs<T>& A, long long w) {
+  const Geo& g = A.g;
+  int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+  int mu = A.mu0 + q;
+  int x[4];
+  coords(g, s, x);
+  M3<T> S, u;
+  zero(S);
 #pragma unroll
-    for (int i = 1; i < 4; i++) {
-      int nu = (mu + i) & 3, p = hyp_pair(mu, nu);
-      add_staples(S, g, x, s, fld<T>(vt, g.vol, p, nu, 4), fld<T>(vt, g.vol, p, mu, 4), mu, nu);
-    }
-    ld(u, U.p[mu], g.vol, s);
-    M3<double> v;
-    lcomb_project(v, a, u, b, S, proj, iter);
-    M3<T> o;
-    cvt(o, v);
-    if (bc == 0 && mu == 0 && x[0] == g.n[0] - 1) zero(o);  // set_bc(), open bc
-    st(U.p[mu], g.vol, s, o);
+  for (int i = 1; i < 4; i++) {
+    int nu = (mu + i) & 3, p = hyp_pair(mu, nu);
+    add_staples(S, g, x, s, fld<T>(A.aux1, g.vol, p, nu, 4), fld<T>(A.aux1, g.vol, p, mu, 4), mu,
+                nu);
   }
+  ld(u, A.U.p[mu], g.vol, s);
+  M3<double> v;
+  lcomb_project(v, A.a, u, A.b, S, A.proj, A.iter);
+  M3<T> o;
+  cvt(o, v);
+  if (A.bc == 0 && mu == 0 && x[0] == g.n[0] - 1) zero(o);  // set_bc(), open bc
+  st(A.U.p[mu], g.vol, s, o);
 }
 
-// ---------------------------------------------------------------------------
 // One APE sweep (ape_links_all, ape_links.c:217-272):
-//   dst(x,mu) = P[src(x,mu) + alpha * sum_{eta != mu} S_eta(src)]
-// ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(128) k_ape(Geo g, Links<T> src, Links<T> dst, double alpha,
-                                             int proj, int iter, int mu0) {
-  const int nd = 4 - mu0;
-  const long long n = (long long)nd * g.vol;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
-       w += (long long)gridDim.x * blockDim.x) {
-    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
-    int mu = mu0 + q;
-    int x[4];
-    coords(g, s, x);
-    M3<T> S, u;
-    zero(S);
-    for (int eta = mu0; eta < 4; eta++) {
-      if (eta == mu) continue;
-      add_staples(S, g, x, s, src.p[eta], src.p[mu], mu, eta);
-    }
-    ld(u, src.p[mu], g.vol, s);
-    M3<double> v;
-#pragma unroll
-    for (int k = 0; k < 9; k++) {  // _su3_mulr then _su3_add (:246-247)
-      double sr = alpha * (double)S.e[k].x, si = alpha * (double)S.e[k].y;
-      v.e[k].x = (double)u.e[k].x + sr;
-      v.e[k].y = (double)u.e[k].y + si;
-    }
-    if (proj) project(v, iter);
-    M3<T> o;
-    cvt(o, v);
-    st(dst.p[mu], g.vol, s, o);
+//   D(x,mu) = P[U(x,mu) + alpha * sum_{eta != mu} S_eta(U)];  w in [0, (4-mu0) V)
+template <class T> __device__ __forceinline__ void ape_item(const SArgs<T>& A, long long w) {
+  const Geo& g = A.g;
+  int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+  int mu = A.mu0 + q;
+  int x[4];
+  coords(g, s, x);
+  M3<T> S, u;
+  zero(S);
+  for (int eta = A.mu0; eta < 4; eta++) {
+    if (eta == mu) continue;
+    add_staples(S, g, x, s, A.U.p[eta], A.U.p[mu], mu, eta);
   }
+  ld(u, A.U.p[mu], g.vol, s);
+  M3<double> v;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {  // _su3_mulr then _su3_add (:246-247)
+    double sr = A.a * (double)S.e[k].x, si = A.a * (double)S.e[k].y;
+    v.e[k].x = (double)u.e[k].x + sr;
+    v.e[k].y = (double)u.e[k].y + si;
+  }
+  if (A.proj) project(v, A.iter);
+  M3<T> o;
+  cvt(o, v);
+  st(A.D.p[mu], g.vol, s, o);
 }
 
-// ---------------------------------------------------------------------------
 // Spatial HYP, level with alpha2 (decorated_links1, hyp_spatial_links.c:210-265)
-//   dl[slot(mu,eta)](x,mu) = P[(1-a2) U + a2/2 S_eta(U)]
-// ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(128) k_hyp3_l1(Geo g, Links<T> U, typename V2<T>::t* dl,
-                                                 double a, double b, int proj, int iter) {
-  const long long n = 6LL * g.vol;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
-       w += (long long)gridDim.x * blockDim.x) {
-    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
-    int mu = 1 + q / 2, eta = ((mu + q % 2) % 3) + 1;
-    int x[4];
-    coords(g, s, x);
-    M3<T> S, u;
-    zero(S);
-    add_staples(S, g, x, s, U.p[eta], U.p[mu], mu, eta);
-    ld(u, U.p[mu], g.vol, s);
-    M3<double> v;
-    lcomb_project(v, a, u, b, S, proj, iter);
-    M3<T> o;
-    cvt(o, v);
-    st(fld<T>(dl, g.vol, hyp3_slot(mu, eta), mu - 1, 3), g.vol, s, o);
+//   dl[slot(mu,eta)](x,mu) = P[(1-a2) U + a2/2 S_eta(U)];  w in [0, 6V)
+template <class T> __device__ __forceinline__ void hyp3_l1_item(const SArgs<T>& A, long long w) {
+  const Geo& g = A.g;
+  int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+  int mu = 1 + q / 2, eta = ((mu + q % 2) % 3) + 1;
+  int x[4];
+  coords(g, s, x);
+  M3<T> S, u;
+  zero(S);
+  add_staples(S, g, x, s, A.U.p[eta], A.U.p[mu], mu, eta);
+  ld(u, A.U.p[mu], g.vol, s);
+  M3<double> v;
+  lcomb_project(v, A.a, u, A.b, S, A.proj, A.iter);
+  M3<T> o;
+  cvt(o, v);
+  st(fld<T>(A.aux0, g.vol, hyp3_slot(mu, eta), mu - 1, 3), g.vol, s, o);
+}
+
+// Spatial HYP, level with alpha1 (decorated_links2, hyp_spatial_links.c:160-207),
+// in place on D (lcomb with D's own link);  w in [0, 3V)
+template <class T> __device__ __forceinline__ void hyp3_l2_item(const SArgs<T>& A, long long w) {
+  const Geo& g = A.g;
+  int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+  int mu = 1 + q;
+  int x[4];
+  coords(g, s, x);
+  M3<T> S, u;
+  zero(S);
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    int nu = ((mu + i) % 3) + 1;
+    add_staples(S, g, x, s, fld<T>(A.aux0, g.vol, hyp3_slot(nu, mu), nu - 1, 3),
+                fld<T>(A.aux0, g.vol, hyp3_slot(mu, nu), mu - 1, 3), mu, nu);
+  }
+  ld(u, A.D.p[mu], g.vol, s);
+  M3<double> v;
+  lcomb_project(v, A.a, u, A.b, S, A.proj, A.iter);
+  M3<T> o;
+  cvt(o, v);
+  st(A.D.p[mu], g.vol, s, o);
+}
+
+#define WLG_GRID_STRIDE(n) \
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < (n); \
+       w += (long long)gridDim.x * blockDim.x)
+
+// batched: one grid over the flattened work of n lattices
+template <class T, int STAGE>
+__global__ void __launch_bounds__(128) kb_smear(const SArgs<T>* __restrict__ A,
+                                                const long long* __restrict__ pre, int n,
+                                                long long total) {
+  WLG_GRID_STRIDE(total) {
+    const int c = find_item(pre, n, w);
+    const long long lw = w - __ldg(pre + c);
+    if (STAGE == BATCH_HYP3) hyp_l3_item<T>(A[c], lw);
+    if (STAGE == BATCH_HYP2) hyp_l2_item<T>(A[c], lw);
+    if (STAGE == BATCH_HYP1) hyp_l1_item<T>(A[c], lw);
+    if (STAGE == BATCH_APE) ape_item<T>(A[c], lw);
+    if (STAGE == BATCH_HYP3D1) hyp3_l1_item<T>(A[c], lw);
+    if (STAGE == BATCH_HYP3D2) hyp3_l2_item<T>(A[c], lw);
   }
 }
 
-// Spatial HYP, level with alpha1 (decorated_links2, hyp_spatial_links.c:160-207)
-template <class T>
-__global__ void __launch_bounds__(128) k_hyp3_l2(Geo g, Links<T> U, const typename V2<T>::t* dl_,
-                                                 double a, double b, int proj, int iter) {
-  const long long n = 3LL * g.vol;
-  typename V2<T>::t* dl = const_cast<typename V2<T>::t*>(dl_);
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
-       w += (long long)gridDim.x * blockDim.x) {
-    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
-    int mu = 1 + q;
-    int x[4];
-    coords(g, s, x);
-    M3<T> S, u;
-    zero(S);
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-      int nu = ((mu + i) % 3) + 1;
-      add_staples(S, g, x, s, fld<T>(dl, g.vol, hyp3_slot(nu, mu), nu - 1, 3),
-                  fld<T>(dl, g.vol, hyp3_slot(mu, nu), mu - 1, 3), mu, nu);
-    }
-    ld(u, U.p[mu], g.vol, s);
-    M3<double> v;
-    lcomb_project(v, a, u, b, S, proj, iter);
-    M3<T> o;
-    cvt(o, v);
-    st(U.p[mu], g.vol, s, o);
-  }
+template <class T> __global__ void __launch_bounds__(128) k_hyp_l3(SArgs<T> A) {
+  WLG_GRID_STRIDE(12LL * A.g.vol) hyp_l3_item<T>(A, w);
+}
+template <class T> __global__ void __launch_bounds__(128) k_hyp_l2(SArgs<T> A) {
+  WLG_GRID_STRIDE(12LL * A.g.vol) hyp_l2_item<T>(A, w);
+}
+template <class T> __global__ void __launch_bounds__(128) k_hyp_l1(SArgs<T> A) {
+  WLG_GRID_STRIDE((long long)A.nmu * A.g.vol) hyp_l1_item<T>(A, w);
+}
+template <class T> __global__ void __launch_bounds__(128) k_ape(SArgs<T> A) {
+  WLG_GRID_STRIDE((long long)(4 - A.mu0) * A.g.vol) ape_item<T>(A, w);
+}
+template <class T> __global__ void __launch_bounds__(128) k_hyp3_l1(SArgs<T> A) {
+  WLG_GRID_STRIDE(6LL * A.g.vol) hyp3_l1_item<T>(A, w);
+}
+template <class T> __global__ void __launch_bounds__(128) k_hyp3_l2(SArgs<T> A) {
+  WLG_GRID_STRIDE(3LL * A.g.vol) hyp3_l2_item<T>(A, w);
 }
 
 // staple_sum: vb(x,mu) += up + down staples in the (mu,nu) plane
@@ -388,18 +392,38 @@ void staples_lnks(int n, const double* u1, const double* u2, const double* u3, d
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+template <class T> static SArgs<T> sargs(const Geo& g) {
+  SArgs<T> A;
+  memset(&A, 0, sizeof(A));
+  A.g = g;
+  return A;
+}
+
 template <class T>
 void hyp_level3(const Geo& g, Links<T> U, typename V2<T>::t* vbar, double a3, int proj, int iter,
                 cudaStream_t st) {
-  k_hyp_l3<T><<<grid_for(12LL * g.vol, 128), 128, 0, st>>>(g, U, vbar, 1.0 - a3, a3 / 2.0, proj,
-                                                           iter);
+  SArgs<T> A = sargs<T>(g);
+  A.U = U;
+  A.aux0 = vbar;
+  A.a = 1.0 - a3;
+  A.b = a3 / 2.0;
+  A.proj = proj;
+  A.iter = iter;
+  k_hyp_l3<T><<<grid_for(12LL * g.vol, 128), 128, 0, st>>>(A);
   WLG_LAUNCH_CHECK("hyp_level3");
 }
 template <class T>
 void hyp_level2(const Geo& g, Links<T> U, const typename V2<T>::t* vbar, typename V2<T>::t* vtil,
                 double a2, int proj, int iter, cudaStream_t st) {
-  k_hyp_l2<T><<<grid_for(12LL * g.vol, 128), 128, 0, st>>>(g, U, vbar, vtil, 1.0 - a2, a2 / 4.0,
-                                                           proj, iter);
+  SArgs<T> A = sargs<T>(g);
+  A.U = U;
+  A.aux0 = const_cast<typename V2<T>::t*>(vbar);
+  A.aux1 = vtil;
+  A.a = 1.0 - a2;
+  A.b = a2 / 4.0;
+  A.proj = proj;
+  A.iter = iter;
+  k_hyp_l2<T><<<grid_for(12LL * g.vol, 128), 128, 0, st>>>(A);
   WLG_LAUNCH_CHECK("hyp_level2");
 }
 template <class T>
@@ -407,29 +431,75 @@ void hyp_level1(const Geo& g, Links<T> U, const typename V2<T>::t* vtil, double 
                 int iter, int mu0, int mu1, int bc, cudaStream_t st) {
   int nmu = mu1 - mu0;
   if (nmu <= 0) return;
-  k_hyp_l1<T><<<grid_for((long long)nmu * g.vol, 128), 128, 0, st>>>(g, U, vtil, 1.0 - a1, a1 / 6.0,
-                                                                     proj, iter, mu0, nmu, bc);
+  SArgs<T> A = sargs<T>(g);
+  A.U = U;
+  A.aux1 = const_cast<typename V2<T>::t*>(vtil);
+  A.a = 1.0 - a1;
+  A.b = a1 / 6.0;
+  A.proj = proj;
+  A.iter = iter;
+  A.mu0 = mu0;
+  A.nmu = nmu;
+  A.bc = bc;
+  k_hyp_l1<T><<<grid_for((long long)nmu * g.vol, 128), 128, 0, st>>>(A);
   WLG_LAUNCH_CHECK("hyp_level1");
 }
 template <class T>
 void ape_sweep(const Geo& g, Links<T> src, Links<T> dst, double alpha, int proj, int iter, int mu0,
                cudaStream_t st) {
-  k_ape<T><<<grid_for((long long)(4 - mu0) * g.vol, 128), 128, 0, st>>>(g, src, dst, alpha, proj,
-                                                                          iter, mu0);
+  SArgs<T> A = sargs<T>(g);
+  A.U = src;
+  A.D = dst;
+  A.a = alpha;
+  A.proj = proj;
+  A.iter = iter;
+  A.mu0 = mu0;
+  k_ape<T><<<grid_for((long long)(4 - mu0) * g.vol, 128), 128, 0, st>>>(A);
   WLG_LAUNCH_CHECK("ape_sweep");
 }
 template <class T>
 void hyp3d_level1(const Geo& g, Links<T> U, typename V2<T>::t* dl, double a2, int proj, int iter,
                   cudaStream_t st) {
-  k_hyp3_l1<T><<<grid_for(6LL * g.vol, 128), 128, 0, st>>>(g, U, dl, 1.0 - a2, a2 / 2.0, proj, iter);
+  SArgs<T> A = sargs<T>(g);
+  A.U = U;
+  A.aux0 = dl;
+  A.a = 1.0 - a2;
+  A.b = a2 / 2.0;
+  A.proj = proj;
+  A.iter = iter;
+  k_hyp3_l1<T><<<grid_for(6LL * g.vol, 128), 128, 0, st>>>(A);
   WLG_LAUNCH_CHECK("hyp3d_level1");
 }
 template <class T>
 void hyp3d_level2(const Geo& g, Links<T> U, const typename V2<T>::t* dl, double a1, int proj,
                   int iter, cudaStream_t st) {
-  k_hyp3_l2<T><<<grid_for(3LL * g.vol, 128), 128, 0, st>>>(g, U, dl, 1.0 - a1, a1 / 4.0, proj, iter);
+  SArgs<T> A = sargs<T>(g);
+  A.D = U;
+  A.aux0 = const_cast<typename V2<T>::t*>(dl);
+  A.a = 1.0 - a1;
+  A.b = a1 / 4.0;
+  A.proj = proj;
+  A.iter = iter;
+  k_hyp3_l2<T><<<grid_for(3LL * g.vol, 128), 128, 0, st>>>(A);
   WLG_LAUNCH_CHECK("hyp3d_level2");
 }
+template <class T>
+void smear_batch(int stage, const SArgs<T>* A, const long long* pre, int n, long long total,
+                 cudaStream_t st) {
+  if (n <= 0 || total <= 0) return;
+  const int grid = grid_for(total, 128);
+  switch (stage) {
+    case BATCH_HYP3: kb_smear<T, BATCH_HYP3><<<grid, 128, 0, st>>>(A, pre, n, total); break;
+    case BATCH_HYP2: kb_smear<T, BATCH_HYP2><<<grid, 128, 0, st>>>(A, pre, n, total); break;
+    case BATCH_HYP1: kb_smear<T, BATCH_HYP1><<<grid, 128, 0, st>>>(A, pre, n, total); break;
+    case BATCH_APE: kb_smear<T, BATCH_APE><<<grid, 128, 0, st>>>(A, pre, n, total); break;
+    case BATCH_HYP3D1: kb_smear<T, BATCH_HYP3D1><<<grid, 128, 0, st>>>(A, pre, n, total); break;
+    case BATCH_HYP3D2: kb_smear<T, BATCH_HYP3D2><<<grid, 128, 0, st>>>(A, pre, n, total); break;
+    default: set_error("smear_batch: unknown stage %d", stage); return;
+  }
+  WLG_LAUNCH_CHECK("smear_batch");
+}
+
 template <class T>
 void staple_sum(const Geo& g, Links<T> u1, Links<T> u2, int mu, int nu, Links<T> vb,
                 cudaStream_t st) {
@@ -460,7 +530,8 @@ void plaq_sum(const Geo& g, int bc, Links<T> U, double* partial, double* out, cu
   template void hyp3d_level2<T>(const Geo&, Links<T>, const V2<T>::t*, double, int, int,          \
                                 cudaStream_t);                                                    \
   template void staple_sum<T>(const Geo&, Links<T>, Links<T>, int, int, Links<T>, cudaStream_t);  \
-  template void plaq_sum<T>(const Geo&, int, Links<T>, double*, double*, cudaStream_t);
+  template void plaq_sum<T>(const Geo&, int, Links<T>, double*, double*, cudaStream_t);    \
+  template void smear_batch<T>(int, const SArgs<T>*, const long long*, int, long long, cudaStream_t);
 
 WLG_INST(double)
 WLG_INST(float)
