@@ -386,7 +386,7 @@ def run_batch(args):
             "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": "c4 batch, HYP2 + APE 0.5 nss 0 5 5 5, r,t <= Ns/2, one graph "
                                    "launch per step", "precision": prec,
-                       "contract_shape_GSBblocknCB": list(shape),
+                       "contract_shape_G_SB_block_nCB": list(shape),
                        "device_bytes": b.device_bytes},
             "kernels_per_graph": kern, "gpu_launches_device_side": kern * args.steps,
             "host_launch_calls": launch_count() - l0,

@@ -53,9 +53,8 @@ def candidates(msl: int, fp64: bool, batched: bool) -> List[Shape]:
     for G in gs:
         if fp64 and G > 3:
             continue
-        for SB in (1, 2):
-            if G == 6 and SB == 2:
-                continue
+        # SB 0: fourth form (shared-memory reduction); 1, 2: third form
+        for SB in ((1,) if G == 6 else (0, 1, 2)):
             for block in ((64,) if fp64 else (64, 128)):
                 out.append((G, SB, block, 0))
     return out
@@ -77,12 +76,12 @@ def tune_context(ctx, parms, precision: str, reps: int = 1, use_cache: bool = Tr
     key = key_for(precision, [ctx.n], parms)
     if use_cache and cached(key):
         G, SB, block, nCB = cached(key)
-        ctx.set_contract_tuning(3 if G <= 4 else 2, G, SB, nCB, block)
+        ctx.set_contract_tuning(_form(G, SB), G, SB, nCB, block)
         return cached(key)
     ctx.snapshot()
     best, best_t = None, float("inf")
     for (G, SB, block, nCB) in candidates(parms.msl, precision == "fp64", batched=False):
-        ctx.set_contract_tuning(3 if G <= 4 else 2, G, SB, nCB, block)
+        ctx.set_contract_tuning(_form(G, SB), G, SB, nCB, block)
         ctx.restore()
         ctx.measure(parms)  # warm-up
         ctx.reset_kernel_times()
@@ -96,7 +95,7 @@ def tune_context(ctx, parms, precision: str, reps: int = 1, use_cache: bool = Tr
         if t < best_t:
             best, best_t = (G, SB, block, nCB), t
     G, SB, block, nCB = best
-    ctx.set_contract_tuning(3 if G <= 4 else 2, G, SB, nCB, block)
+    ctx.set_contract_tuning(_form(G, SB), G, SB, nCB, block)
     ctx.restore()
     _store(key, best)
     return best
@@ -131,6 +130,11 @@ def tune_batch(batch, reps: int = 1, use_cache: bool = True) -> Shape:
     batch.restore()
     _store(key, best)
     return best
+
+
+def _form(G: int, SB: int) -> int:
+    """kernel form of a shape: 2 for G = 6, 4 for SB = 0, else 3"""
+    return 2 if G > 4 else (4 if SB == 0 else 3)
 
 
 def _as_batch(shape: Shape):

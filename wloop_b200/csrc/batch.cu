@@ -405,8 +405,9 @@ int plan(wlg_batch* b) {
   const bool fp64 = b->prec == WLG_FP64;
   for (Cfg& f : b->cfg) {
     f.cp = contract_plan(f.g, f.p.msl, f.p.mwlt, fp64, b->tG, b->tNCB, b->tBlock);
-    if (b->tSB) f.cp.SB = b->tSB;
-    f.cp.variant = 3;
+    // batched forms: SB = 1 or 2 selects the third form, SB = 0 the fourth
+    f.cp.SB = b->tG ? b->tSB : 0;
+    f.cp.variant = f.cp.SB ? 3 : 4;
     if (f.cp.G > 4) {
       set_error("batch: contraction shape G=%d is not available in batched form", f.cp.G);
       return -1;

@@ -236,11 +236,12 @@ ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hin
   if (G == 5) G = 6;
   p.G = G;
   p.SB = (msl >= 2 && G <= 4 && !(fp64 && G >= 3)) ? 2 : 1;
-  // third form (staged top lines) unless G = 6, which only the second form has
-  p.variant = (G <= 4) ? 3 : 2;
+  // fourth form (staged top lines, shared-memory reduction) unless G = 6,
+  // which only the second form has
+  p.variant = (G <= 4) ? 4 : 2;
   p.ngrp = (msl + G - 1) / G;
   // FP64 stages twice the bytes per thread: 64-thread blocks keep 3 blocks per SM
-  p.block = block_hint > 0 ? block_hint : ((fp64 && p.variant == 3) ? 64 : 128);
+  p.block = block_hint > 0 ? block_hint : ((fp64 && p.variant == 4) ? 64 : 128);
   int ncol = 3 * g.vs;
   int nCB = nCB_hint;
   if (nCB <= 0) {
@@ -498,10 +499,204 @@ static void launch_contract3_sb(const Geo& g, const ContractPlan& p, const typen
     launch_contract3<T, G, 1>(g, p, u0, lines, msl, mwlt, R, partial, st);
 }
 
+// ---------------------------------------------------------------------------
+// contraction kernel, fourth form: the third form with the warp reduction
+// done through shared memory instead of shuffles.  After the recursion a lane
+// forms its G*msl traces one top level at a time; once a level's staged
+// lines are in registers (warp barrier), the lanes write their traces into
+// that level's stage chunks (row (g,s2): 32 doubles, one per lane, in chunk
+// (s2, q=g) shifted by (row & 7) * 16 bytes so that eight consecutive rows
+// fall on distinct banks); after a second barrier lane r adds up row r in FP64
+// and accumulates it.  No shuffles, no dependent reduction chains, and no
+// extra shared memory: the rows reuse the stage of the current step.
+// ---------------------------------------------------------------------------
+template <class T, int G>
+__device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
+  extern __shared__ double acc[];  // [nwarps][mwlt][G][msl] doubles, then the line stage
+  constexpr int NQ = Chunks<T>::N;
+  static_assert(G <= NQ, "one stage chunk per bottom level");
+
+  const Geo& g = A.g;
+  const typename V2<T>::t* __restrict__ u0 = A.u0;
+  const typename V2<T>::t* __restrict__ lines = A.lines;
+  const int msl = A.msl, mwlt = A.mwlt, R = A.R, ngrp = A.ngrp, nCB = A.nCB;
+  double* __restrict__ partial = A.partial;
+  const int N0 = g.n[0], vs = g.vs, vol = g.vol;
+  int b = bid;
+  const int x0 = b % N0;
+  b /= N0;
+  const int grp = b % ngrp;
+  const int cb = b / ngrp;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int rowlen = mwlt * G * msl;
+  double* wacc = acc + (size_t)warp * rowlen;
+  char* stage = reinterpret_cast<char*>(acc + (size_t)nwarps * rowlen);
+  const int qstride = blockDim.x * 16;
+  char* myslot = stage + threadIdx.x * 16;
+  char* wchunks = stage + warp * 32 * 16;  // this warp's part of chunk (s2,q): + (s2*NQ+q)*qstride
+  for (int i = lane; i < rowlen; i += 32) wacc[i] = 0.0;
+  __syncwarp();
+
+  const int s1_0 = grp * G;
+  const int ncol = 3 * vs;
+  const int per = (ncol + nCB - 1) / nCB;
+  const int c_begin = cb * per;
+  const int c_end = min(ncol, c_begin + per);
+  const size_t fstride = link_elems<T>(vol);
+  const int nrows = G * msl;
+
+  for (int cbase = c_begin; cbase < c_end; cbase += blockDim.x) {
+    const int col = cbase + threadIdx.x;
+    const bool active = col < c_end;
+    const int cc = active ? col : c_begin;
+    const int k = cc / vs, xs = cc - k * vs;
+    int xsR;
+    {
+      const int x1 = xs / g.st[1], r = xs - x1 * g.st[1];
+      const int x2 = r / g.st[2], x3 = r - x2 * g.st[2];
+      const int xk = (k == 0) ? x1 : ((k == 1) ? x2 : x3);
+      const int nk = g.n[k + 1];
+      int y = xk + (R % nk);
+      if (y >= nk) y -= nk;
+      xsR = xs + (y - xk) * g.st[k + 1];
+    }
+    const typename V2<T>::t* lk = lines + (size_t)k * fstride;
+    const size_t lvl = 3 * fstride;
+    M3<T> C[G];
+#pragma unroll
+    for (int gi = 0; gi < G; gi++) {
+      int s1 = min(s1_0 + gi, msl - 1);
+      ld(C[gi], lk + (size_t)s1 * lvl, vol, x0 * vs + xs);
+      if (!active) zero(C[gi]);  // idle lanes contribute exact zeros
+    }
+    M3<T> ua, ub;
+    ld(ua, u0, vol, x0 * vs + xs);
+    ld(ub, u0, vol, x0 * vs + xsR);
+    int t0 = x0;
+    for (int tt = 1; tt <= mwlt; tt++) {
+      const int t1 = (t0 + 1 == N0) ? 0 : t0 + 1;  // x0+T mod N0: the top slice
+      const int stop = t1 * vs + xs;
+      __syncwarp();  // previous step's rows are read before the stage is refilled
+      for (int s2 = 0; s2 < msl; s2++) {
+        const typename V2<T>::t* src = lk + (size_t)s2 * lvl;
+#pragma unroll
+        for (int q = 0; q < NQ; q++)
+          cp_async16(myslot + (s2 * NQ + q) * qstride, chunk_ptr<T>(src, stop, q));
+      }
+      cp_async_commit();
+#pragma unroll
+      for (int gi = 0; gi < G; gi++) lmul_dag_inplace(C[gi], ua);
+#pragma unroll
+      for (int gi = 0; gi < G; gi++) rmul_inplace(C[gi], ub);
+      t0 = t1;
+      if (tt < mwlt) {
+        ld(ua, u0, vol, t0 * vs + xs);
+        ld(ub, u0, vol, t0 * vs + xsR);
+      }
+      cp_async_wait_all();
+#pragma unroll 1
+      for (int s2 = 0; s2 < msl; s2++) {
+        M3<T> l;
+        ld_stage<T>(l, myslot + s2 * NQ * qstride, qstride);
+        __syncwarp();  // every lane holds level s2 before its chunks are overwritten
+#pragma unroll
+        for (int gi = 0; gi < G; gi++) {
+          const int row = gi * msl + s2;
+          double* dst = reinterpret_cast<double*>(wchunks + (s2 * NQ + gi) * qstride + (row & 7) * 16);
+          dst[lane] = (double)retr_dag(l, C[gi]);
+        }
+      }
+      __syncwarp();
+      double* arow = wacc + (size_t)(tt - 1) * nrows;
+      for (int row = lane; row < nrows; row += 32) {
+        const int gi = row / msl, s2 = row - gi * msl;
+        const double2* src =
+            reinterpret_cast<const double2*>(wchunks + (s2 * NQ + gi) * qstride + (row & 7) * 16);
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          double2 v = src[j];
+          s0 += v.x;
+          s1 += v.y;
+        }
+        arow[row] += s0 + s1;
+      }
+    }
+  }
+  __syncthreads();
+  double* out = partial + ((size_t)(x0 * ngrp + grp) * nCB + cb) * rowlen;
+  for (int i = threadIdx.x; i < rowlen; i += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < nwarps; w++) s += acc[(size_t)w * rowlen + i];
+    out[i] = s;
+  }
+}
+
+template <class T, int G, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_contract4(CArgs<T> A) {
+  contract4_body<T, G>(A, blockIdx.x);
+}
+
+template <class T, int G, int MINB>
+__global__ void __launch_bounds__(128, MINB) kb_contract4(const CArgs<T>* __restrict__ A,
+                                                          const long long* __restrict__ pre, int n) {
+  const int c = find_item(pre, n, (long long)blockIdx.x);
+  contract4_body<T, G>(A[c], (int)(blockIdx.x - pre[c]));
+}
+
+template <class T, int G>
+static void launch_contract4(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
+                             const typename V2<T>::t* lines, int msl, int mwlt, int R,
+                             double* partial, cudaStream_t st) {
+  constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
+  auto kern = k_contract4<T, G, MINB>;
+  size_t smem = contract3_smem<T>(p, msl);
+  static size_t smem_set = 48 * 1024;
+  if (smem > smem_set) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_set = smem;
+  }
+  CArgs<T> A;
+  A.g = g;
+  A.u0 = u0;
+  A.lines = lines;
+  A.msl = msl;
+  A.mwlt = mwlt;
+  A.R = R;
+  A.ngrp = p.ngrp;
+  A.nCB = p.nCB;
+  A.partial = partial;
+  kern<<<g.n[0] * p.ngrp * p.nCB, p.block, smem, st>>>(A);
+  WLG_LAUNCH_CHECK("contract");
+}
+
+template <class T, int G>
+static void launch_contract4_batch(const CArgs<T>* A, const long long* pre, int n, long long nblocks,
+                                   int block, size_t smem, cudaStream_t st) {
+  constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
+  auto kern = kb_contract4<T, G, MINB>;
+  static size_t smem_set = 48 * 1024;
+  if (smem > smem_set) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_set = smem;
+  }
+  kern<<<(unsigned)nblocks, block, smem, st>>>(A, pre, n);
+  WLG_LAUNCH_CHECK("contract_batch");
+}
+
 template <class T>
 void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
               const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
               cudaStream_t st) {
+  if (p.variant == 4) {
+    switch (p.G) {
+      case 1: launch_contract4<T, 1>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      case 2: launch_contract4<T, 2>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      case 3: launch_contract4<T, 3>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      case 4: launch_contract4<T, 4>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      default: break;
+    }
+  }
   if (p.variant == 3) {
     switch (p.G) {
       case 1: launch_contract3_sb<T, 1>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
@@ -616,6 +811,14 @@ template <class T>
 void contract_batch(int G, int SB, const CArgs<T>* A, const long long* pre, int n, long long nblocks,
                     int block, size_t smem, cudaStream_t st) {
   if (n <= 0 || nblocks <= 0) return;
+  if (SB == 0) {  // fourth form (shared-memory reduction)
+    switch (G) {
+      case 1: launch_contract4_batch<T, 1>(A, pre, n, nblocks, block, smem, st); return;
+      case 2: launch_contract4_batch<T, 2>(A, pre, n, nblocks, block, smem, st); return;
+      case 3: launch_contract4_batch<T, 3>(A, pre, n, nblocks, block, smem, st); return;
+      case 4: launch_contract4_batch<T, 4>(A, pre, n, nblocks, block, smem, st); return;
+    }
+  }
   if (SB == 2) {
     switch (G) {
       case 1: launch_contract3_batch<T, 1, 2>(A, pre, n, nblocks, block, smem, st); return;
