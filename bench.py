@@ -191,23 +191,9 @@ def run_ours(args, rank, world, local):
     from wloop_b200.api import Context, launch_count, peak_tflops
     from wloop_b200.workloads import C3, flops_per_config
 
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-    def barrier_max(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
+    from wloop_b200.replicas import Replicas
+    rep = Replicas(backend="nccl" if world > 1 else None)
+    barrier_max, barrier = rep.max, rep.barrier
 
     w = C3
     if args.lattice:
@@ -341,9 +327,7 @@ def run_ours(args, rank, world, local):
                 "gpu_launches": launches, "fp64_form": fp64, "kernel_share": shares,
                 "algorithmic_flops_per_config": fl["total"]}
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
 
 
 def run_batch(args):

@@ -234,7 +234,8 @@ int wlg_reset_kernel_times(wlg_ctx* ctx);
  * threads (multiple of 32, at most 128). */
 int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
 /* As above plus the kernel form (2: register-prefetching, 3: staged top
- * lines) and SB top levels per reduction (1 or 2). */
+ * lines, shuffle reduction; 4: staged top lines, shared-memory reduction) and
+ * SB top levels per reduction (1 or 2; form 3 only). */
 int wlg_set_contract_tuning(wlg_ctx* ctx, int variant, int G, int SB, int nCB, int block);
 /* The context's CUDA stream (cudaStream_t), for callers that record events. */
 void* wlg_stream(wlg_ctx* ctx);
@@ -247,6 +248,26 @@ int wlg_restore(wlg_ctx* ctx);
 /* Achievable vector FMA throughput of the device in TFLOP/s (2 flops per
  * FMA), FP64 or FP32 (precision WLG_FP64 / WLG_MIXED). */
 int wlg_peak_flops(int precision, int device, double* tflops);
+
+/* ---- measurement output files (host only) -----------------------------------
+ * .dat of the measurement program (main/ms10.c:86-190): head = 5 int32
+ * {wls, msl, mwlt, mwlr, tmax}, then per configuration int32 nc and wls
+ * doubles (wl_mat, index wl_idx), little-endian.  These replace ms10's static
+ * write_file_head / check_file_head / write_data / read_data.  Errors return
+ * -1 with the message in wlg_dat_error(). */
+const char* wlg_dat_error(void);
+/* head of a measurement with parameters p on a lattice of time extent n0 */
+int wlg_dat_head(const wlg_wloop_parms* p, int n0, int head[5]);
+int wlg_dat_write_head(const char* path, const int head[5]);   /* creates / truncates */
+int wlg_dat_check_head(const char* path, const int head[5]);
+int wlg_dat_append(const char* path, int nc, const double* wl_mat, int wls);
+/* complete records in the file (head copied out); -1 on a torn last record */
+long long wlg_dat_count(const char* path, int head[5]);
+int wlg_dat_read(const char* path, long long rec, int* nc, double* wl_mat, int wls);
+/* wloop part of the .par file (wloop_parms.c:343-382): appended to path /
+ * compared with the record at byte offset `offset`. */
+int wlg_par_write_wloop(const char* path, const wlg_wloop_parms* p);
+int wlg_par_check_wloop(const char* path, long long offset, const wlg_wloop_parms* p);
 
 #ifdef __cplusplus
 }

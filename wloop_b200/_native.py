@@ -117,6 +117,15 @@ def _load():
         "wlg_server_stats": (i, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                  C.POINTER(C.c_longlong), dp, dp, dp]),
         "wlg_server_budget": (C.c_longlong, [vp]),
+        "wlg_dat_error": (C.c_char_p, []),
+        "wlg_dat_head": (i, [C.POINTER(WlgParms), i, ip]),
+        "wlg_dat_write_head": (i, [C.c_char_p, ip]),
+        "wlg_dat_check_head": (i, [C.c_char_p, ip]),
+        "wlg_dat_append": (i, [C.c_char_p, i, dp, i]),
+        "wlg_dat_count": (C.c_longlong, [C.c_char_p, ip]),
+        "wlg_dat_read": (i, [C.c_char_p, C.c_longlong, ip, dp, i]),
+        "wlg_par_write_wloop": (i, [C.c_char_p, C.POINTER(WlgParms)]),
+        "wlg_par_check_wloop": (i, [C.c_char_p, C.c_longlong, C.POINTER(WlgParms)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

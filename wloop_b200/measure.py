@@ -1,0 +1,255 @@
+"""Measurement runs over a list of configurations, as main/ms10.c does them.
+
+ms10 (main/ms10.c:687-760) visits the configurations first, first+step, ...,
+last; for each it HYP-smears the gauge field with alpha_action and computes
+the Wilson-loop matrices (set_data, ms10.c:633-646), then appends one record
+to its .dat file (save_data, ms10.c:649-659).  `run` does the same on the GPU
+through the C ABI and writes the same .dat format (head and records through
+wlg_dat_* of libwloop_b200.so) plus the wloop part of the .par file.
+
+Several processes (one per GPU, launched by torchrun) share a run as
+replicas: rank r measures every world-th configuration into its own file
+<name>.r<rank>.dat, and `merge` interleaves those into the single
+<name>.dat ordered by configuration number that one process would have
+written.  No device data crosses ranks.
+
+Configurations come from a callable nc -> host field (complex128, shape
+(V, 4, 3, 3), su3_dble layout) or, without one, are synthetic fields
+generated on the device with seed nc.  Reading openQCD's exported
+configuration files belongs to openQCD and is not part of this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+from dataclasses import dataclass
+from typing import Callable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from ._native import WlgError, dptr, iptr, lib
+from .api import Context, WloopParms
+from .replicas import Replicas, config_numbers, shard
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise WlgError(f"{what}: {lib.wlg_dat_error().decode(errors='replace')}")
+
+
+def _b(path: str) -> bytes:
+    return os.fsencode(path)
+
+
+# ---------------------------------------------------------------------------
+# .dat and .par files
+# ---------------------------------------------------------------------------
+def dat_head(p: WloopParms, n0: int) -> List[int]:
+    """[wls, msl, mwlt, mwlr, tmax] of a run (ms10.c:86-105)."""
+    h = (C.c_int * 5)()
+    cp = p.to_c()
+    _check(lib.wlg_dat_head(C.byref(cp), n0, h), "dat_head")
+    return list(h)
+
+
+def write_head(path: str, head: Sequence[int]) -> None:
+    _check(lib.wlg_dat_write_head(_b(path), (C.c_int * 5)(*head)), "write_file_head")
+
+
+def check_head(path: str, head: Sequence[int]) -> None:
+    _check(lib.wlg_dat_check_head(_b(path), (C.c_int * 5)(*head)), "check_file_head")
+
+
+def append(path: str, nc: int, wl: np.ndarray) -> None:
+    wl = np.ascontiguousarray(wl, dtype=np.float64)
+    _check(lib.wlg_dat_append(_b(path), int(nc), dptr(wl), wl.size), "write_data")
+
+
+def count(path: str) -> Tuple[List[int], int]:
+    """(head, number of complete records)."""
+    h = (C.c_int * 5)()
+    n = lib.wlg_dat_count(_b(path), h)
+    if n < 0:
+        _check(-1, "read_data")
+    return list(h), int(n)
+
+
+def read(path: str) -> Tuple[List[int], np.ndarray, np.ndarray]:
+    """(head, nc of every record, wl_mat of every record as (records, wls))."""
+    head, n = count(path)
+    wls = head[0]
+    ncs = np.empty(n, dtype=np.int32)
+    wl = np.empty((n, wls), dtype=np.float64)
+    nc = C.c_int()
+    for r in range(n):
+        _check(lib.wlg_dat_read(_b(path), r, C.byref(nc), dptr(wl[r]), wls), "read_data")
+        ncs[r] = nc.value
+    return head, ncs, wl
+
+
+def merge(parts: Sequence[str], out: str) -> int:
+    """Interleaves per-replica .dat files into one, ordered by configuration
+    number (stable for repeated numbers).  All parts must share one head.
+    Returns the number of records written."""
+    head = None
+    recs = []
+    for i, path in enumerate(parts):
+        h, ncs, wl = read(path)
+        if head is None:
+            head = h
+        elif h != head:
+            raise WlgError(f"merge: {path} has head {h}, expected {head}")
+        recs.extend((int(nc), i, r, wl[r]) for r, nc in enumerate(ncs))
+    if head is None:
+        raise WlgError("merge: no input files")
+    recs.sort(key=lambda x: (x[0], x[1], x[2]))
+    write_head(out, head)
+    for nc, _, _, w in recs:
+        append(out, nc, w)
+    return len(recs)
+
+
+def write_par(path: str, p: WloopParms) -> None:
+    """Appends the wloop record of the .par file (wloop_parms.c:343-382)."""
+    cp = p.to_c()
+    _check(lib.wlg_par_write_wloop(_b(path), C.byref(cp)), "write_wloop_parms")
+
+
+def check_par(path: str, p: WloopParms, offset: int = 0) -> None:
+    cp = p.to_c()
+    _check(lib.wlg_par_check_wloop(_b(path), offset, C.byref(cp)), "check_wloop_parms")
+
+
+# ---------------------------------------------------------------------------
+# runs
+# ---------------------------------------------------------------------------
+@dataclass
+class Run:
+    """One measurement run (the [Run name], [Configurations] and [Wloop]
+    sections of ms10's input file, plus the lattice)."""
+    name: str
+    n: Tuple[int, int, int, int]
+    bc: int
+    parms: WloopParms
+    first: int
+    last: int
+    step: int = 1
+    precision: str = "mixed"
+    eps: float = 0.2  # synthetic fields only
+
+    @property
+    def configs(self) -> List[int]:
+        return config_numbers(self.first, self.last, self.step)
+
+
+def dat_path(out_dir: str, name: str, rank: int = 0, world: int = 1) -> str:
+    if world == 1:
+        return os.path.join(out_dir, f"{name}.dat")
+    return os.path.join(out_dir, f"{name}.r{rank}.dat")
+
+
+def _device_measure(run: Run, source, device: int):
+    ctx = Context(run.n, run.bc, run.precision, device=device)
+
+    def measure(nc: int) -> np.ndarray:
+        if source is None:
+            ctx.generate(nc, run.eps)
+        else:
+            ctx.upload(source(nc))
+        return ctx.measure(run.parms)
+
+    return ctx, measure
+
+
+def run(r: Run, out_dir: str, replicas: Optional[Replicas] = None,
+        source: Optional[Callable[[int], np.ndarray]] = None,
+        measure: Optional[Callable[[int], np.ndarray]] = None,
+        log: Optional[Callable[[str], None]] = None) -> dict:
+    """Measures this rank's share of the run's configurations and appends one
+    record per configuration to its .dat file.  `measure` (nc -> wl_mat)
+    replaces the device measurement; by default a Context on this rank's
+    local GPU runs HYP(alpha_action) + wloop_sum on each configuration.
+    With several replicas, rank 0 merges the per-rank files into
+    <name>.dat after all ranks have finished."""
+    rank = replicas.rank if replicas else 0
+    world = replicas.world if replicas else 1
+    local = replicas.local if replicas else 0
+    os.makedirs(out_dir, exist_ok=True)
+    head = dat_head(r.parms, r.n[0])
+    path = dat_path(out_dir, r.name, rank, world)
+    write_head(path, head)
+    if rank == 0:
+        par = os.path.join(out_dir, f"{r.name}.par")
+        if os.path.exists(par):
+            os.remove(par)
+        write_par(par, r.parms)
+    mine = shard(r.configs, rank, world)
+    ctx = None
+    if measure is None:
+        ctx, measure = _device_measure(r, source, local)
+    seconds = []
+    try:
+        for nc in mine:
+            t0 = time.perf_counter()
+            wl = measure(nc)
+            if wl.size != head[0]:
+                raise WlgError(f"measurement of configuration {nc} has {wl.size} entries, "
+                               f"expected {head[0]}")
+            append(path, nc, wl)
+            seconds.append(time.perf_counter() - t0)
+            if log:
+                log(f"Configuration no {nc} fully processed in {seconds[-1]:.2e} sec")
+    finally:
+        if ctx is not None:
+            ctx.close()
+    out = {"rank": rank, "world": world, "path": path, "configs": mine, "seconds": seconds}
+    if world > 1:
+        replicas.barrier()
+        if rank == 0:
+            parts = [dat_path(out_dir, r.name, k, world) for k in range(world)]
+            out["merged"] = os.path.join(out_dir, f"{r.name}.dat")
+            out["records"] = merge(parts, out["merged"])
+        replicas.barrier()
+    return out
+
+
+def main(argv=None) -> int:
+    """Command line: python -m wloop_b200.measure --name run1 --lattice 64x32x32x32 ...
+    (under torchrun for several GPUs)."""
+    import argparse
+    from .api import APE, HYP
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--name", required=True)
+    ap.add_argument("--out", default=".")
+    ap.add_argument("--lattice", required=True, help="N0xN1xN2xN3")
+    ap.add_argument("--bc", type=int, default=3, help="0 open, 3 periodic")
+    ap.add_argument("--first", type=int, default=1)
+    ap.add_argument("--last", type=int, default=1)
+    ap.add_argument("--step", type=int, default=1)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--eps", type=float, default=0.2)
+    ap.add_argument("--msl", type=int, required=True)
+    ap.add_argument("--nss", type=int, nargs="+", required=True)
+    ap.add_argument("--mwlt", type=int, required=True)
+    ap.add_argument("--mwlr", type=int, required=True)
+    ap.add_argument("--op-smear", default="APE", choices=["APE", "HYP"])
+    ap.add_argument("--alpha-action", type=float, nargs=3, default=(1.0, 1.0, 0.5))
+    ap.add_argument("--alpha", type=float, nargs="+", default=[0.5])
+    ap.add_argument("--proj-iter", type=int, default=4)
+    a = ap.parse_args(argv)
+    n = tuple(int(x) for x in a.lattice.split("x"))
+    hyp = a.op_smear == "HYP"
+    p = WloopParms(a.msl, a.nss, a.mwlt, a.mwlr, HYP if hyp else APE, tuple(a.alpha_action),
+                   0.0 if hyp else a.alpha[0], tuple(a.alpha[:2]) if hyp else (0.0, 0.0),
+                   a.proj_iter)
+    r = Run(a.name, n, a.bc, p, a.first, a.last, a.step, a.precision, a.eps)
+    with Replicas() as rep:
+        res = run(r, a.out, rep, log=print if rep.rank == 0 else None)
+    if res.get("merged"):
+        print(f"{res['records']} records in {res['merged']}")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
