@@ -163,7 +163,9 @@ int wlg_batch_result(wlg_batch* b, int i, double* wl_mat);
 /* device time of the last run and kernels per run */
 int wlg_batch_stats(wlg_batch* b, double* last_ms, int* kernels_per_run);
 void* wlg_batch_stream(wlg_batch* b);
-/* contraction shape for the whole batch (0 = automatic); G <= 4 */
+/* contraction shape for the whole batch (0 = automatic); G <= 4; SB selects
+ * the form: 1 or 2 the third (SB levels per reduction), 0 the fourth, 3 the
+ * fourth with its level loops unrolled (msl 4-6) */
 int wlg_batch_set_contract_shape(wlg_batch* b, int G, int SB, int nCB, int block);
 /* on (default): the first run executes directly and captures the pipeline,
  * later runs replay the graph; off: every run executes directly */
@@ -234,8 +236,9 @@ int wlg_reset_kernel_times(wlg_ctx* ctx);
  * threads (multiple of 32, at most 128). */
 int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
 /* As above plus the kernel form (2: register-prefetching, 3: staged top
- * lines, shuffle reduction; 4: staged top lines, shared-memory reduction) and
- * SB top levels per reduction (1 or 2; form 3 only). */
+ * lines, shuffle reduction; 4: staged top lines, shared-memory reduction;
+ * 5: form 4 with its level loops unrolled for msl 4-6) and SB top levels per
+ * reduction (1 or 2; form 3 only). */
 int wlg_set_contract_tuning(wlg_ctx* ctx, int variant, int G, int SB, int nCB, int block);
 /* The context's CUDA stream (cudaStream_t), for callers that record events. */
 void* wlg_stream(wlg_ctx* ctx);
@@ -245,6 +248,15 @@ long long wlg_launch_count(void);
  * device; lets repeated measurements start from the unsmeared field). */
 int wlg_snapshot(wlg_ctx* ctx);
 int wlg_restore(wlg_ctx* ctx);
+/* Symmetries of the measurement, for invariance checks at full size
+ * (devel/wloop/check2.c, devel/wloop/check3.c; openQCD's transform_ud and
+ * shift_ud).  wlg_gauge_transform: U_mu(x) <- g(x) U_mu(x) g(x+mu)^dag on the
+ * context's gauge field, g(x) a synthetic SU(3) field from (seed, eps) as in
+ * wlg_generate.  wlg_shift_links: U(x) <- U(x - s), periodic; with open
+ * boundary conditions only s[0] = 0 (mod N0) is accepted.  Wilson loops are
+ * unchanged by the first and move to W(x0 - s0) under the second. */
+int wlg_gauge_transform(wlg_ctx* ctx, uint64_t seed, double eps);
+int wlg_shift_links(wlg_ctx* ctx, const int s[4]);
 /* Achievable vector FMA throughput of the device in TFLOP/s (2 flops per
  * FMA), FP64 or FP32 (precision WLG_FP64 / WLG_MIXED). */
 int wlg_peak_flops(int precision, int device, double* tflops);

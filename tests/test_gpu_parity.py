@@ -190,6 +190,16 @@ CASES = [
                                  alpha_ape=0.4, proj_iter=0)),
     ((10, 6, 6, 6), 0, WloopParms(msl=6, nss=[0, 2, 2, 2, 2, 2], mwlt=6, mwlr=4, op_smear=APE,
                                   alpha_ape=0.5, proj_iter=4)),
+    # level counts at the ends of the range (1, 2, 7 and MAX_SM_LEVELS = 8) and
+    # odd extents (time slices of 105 sites, not a multiple of the 32-site tile)
+    ((6, 4, 4, 4), 3, WloopParms(msl=1, nss=[3], mwlt=4, mwlr=3, op_smear=APE, alpha_ape=0.5,
+                                 proj_iter=4)),
+    ((7, 5, 3, 7), 3, WloopParms(msl=2, nss=[0, 2], mwlt=4, mwlr=2, op_smear=APE, alpha_ape=0.5,
+                                 proj_iter=4)),
+    ((6, 4, 6, 4), 0, WloopParms(msl=7, nss=[0, 1, 1, 1, 1, 1, 1], mwlt=4, mwlr=3, op_smear=APE,
+                                 alpha_ape=0.5, proj_iter=4)),
+    ((4, 4, 4, 6), 3, WloopParms(msl=8, nss=[1, 1, 0, 1, 1, 1, 0, 1], mwlt=3, mwlr=3,
+                                 op_smear=HYP, alpha_hyp=(0.6, 0.3), proj_iter=3)),
 ]
 
 
@@ -206,7 +216,7 @@ def test_wloop_sum_fp64(case):
     assert np.abs(plaq - ref_plaq).max() / np.abs(ref_plaq).max() < 1e-12
 
 
-@pytest.mark.parametrize("case", [0, 1, 4])
+@pytest.mark.parametrize("case", [0, 1, 3, 4, 6, 8])
 def test_wloop_sum_mixed(case):
     n, bc, p = CASES[case]
     u = generate_links(n, bc, 100 + case, 0.25)

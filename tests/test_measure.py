@@ -210,7 +210,7 @@ def test_run_on_gpu_matches_context_and_oracle(tmp_path):
             ctx.upload(fields[nc])
             assert np.array_equal(ctx.measure(P), wl[k])
     u = O.hyp_links(N, 0, fields[2], *P.alpha_action, 1, P.proj_iter)
-    ref = O.wloop_sum(N, 0, u, P)[0]
+    ref = O.wloop_sum(N, 0, u, P)
     scale = np.maximum(np.abs(ref), 1.0)
     assert np.max(np.abs(wl[1] - ref) / scale) < 1e-12
 

@@ -90,6 +90,8 @@ def _load():
         "wlg_stream": (vp, [vp]),
         "wlg_launch_count": (C.c_longlong, []),
         "wlg_snapshot": (i, [vp]),
+        "wlg_gauge_transform": (i, [vp, u64, d]),
+        "wlg_shift_links": (i, [vp, ip]),
         "wlg_restore": (i, [vp]),
         "wlg_peak_flops": (i, [i, i, dp]),
         "wlg_batch_create": (i, [i, ip, ip, C.POINTER(WlgParms), i, i, C.POINTER(vp)]),

@@ -234,6 +234,15 @@ class Context:
         """cudaStream_t of the context (for event timing by the caller)."""
         return lib.wlg_stream(self._h) or 0
 
+    def gauge_transform(self, seed: int, eps: float = 1.0):
+        """U_mu(x) <- g(x) U_mu(x) g(x+mu)^dag with a synthetic SU(3) field g
+        (openQCD's random_g + transform_ud, devel/wloop/check2.c)."""
+        check(lib.wlg_gauge_transform(self._h, seed, eps), "gauge_transform")
+
+    def shift_ud(self, s):
+        """U(x) <- U(x - s) (openQCD's shift_ud, devel/wloop/check3.c)."""
+        check(lib.wlg_shift_links(self._h, (C.c_int * 4)(*s)), "shift_ud")
+
     def snapshot(self):
         check(lib.wlg_snapshot(self._h), "snapshot")
 

@@ -42,6 +42,7 @@ struct Op {
   int n;               // lattices in the launch
   long long total;     // work items (blocks for OP_CONTRACT)
   int G, SB, block;    // OP_CONTRACT
+  int msl;             // OP_CONTRACT: level count of every lattice in the launch, 0 if mixed
   size_t smem;
   void* dst;
   const void* src;
@@ -270,7 +271,7 @@ template <class T> void build_ops(wlg_batch* b) {
     std::vector<RArgs> ra;
     std::vector<long long> ru;
     struct Group {
-      int G, SB, block;
+      int G, SB, block, msl;
       size_t smem;
       std::vector<CArgs<T>> a;
       std::vector<long long> blocks;
@@ -307,9 +308,11 @@ template <class T> void build_ops(wlg_batch* b) {
       for (auto& gr : groups)
         if (gr.G == f.cp.G && gr.SB == f.cp.SB && gr.block == f.cp.block) gp = &gr;
       if (!gp) {
-        groups.push_back(Group{f.cp.G, f.cp.SB, f.cp.block, 0, {}, {}});
+        groups.push_back(Group{f.cp.G, f.cp.SB, f.cp.block, f.p.msl, 0, {}, {}});
         gp = &groups.back();
       }
+      // unrolled kernels need one level count for the whole launch
+      if (gp->msl != f.p.msl || f.cp.variant != 5) gp->msl = 0;
       gp->smem = std::max(gp->smem, contract3_smem<T>(f.cp, f.p.msl));
       gp->a.push_back(ca);
       gp->blocks.push_back((long long)f.g.n[0] * f.cp.ngrp * f.cp.nCB);
@@ -337,6 +340,7 @@ template <class T> void build_ops(wlg_batch* b) {
       op.G = gr.G;
       op.SB = gr.SB;
       op.block = gr.block;
+      op.msl = gr.msl;
       op.smem = gr.smem;
       b->ops.push_back(op);
     }
@@ -382,7 +386,7 @@ template <class T> int issue(wlg_batch* b) {
       case OP_CONTRACT:
         contract_batch<T>(op.G, op.SB, (const CArgs<T>*)(b->tables + op.tab),
                           (const long long*)(b->tables + op.pre), op.n, op.total, op.block,
-                          op.smem, b->st);
+                          op.smem, op.msl, b->st);
         kernels++;
         break;
       case OP_REDUCE:
@@ -405,9 +409,10 @@ int plan(wlg_batch* b) {
   const bool fp64 = b->prec == WLG_FP64;
   for (Cfg& f : b->cfg) {
     f.cp = contract_plan(f.g, f.p.msl, f.p.mwlt, fp64, b->tG, b->tNCB, b->tBlock);
-    // batched forms: SB = 1 or 2 selects the third form, SB = 0 the fourth
+    // batched forms: SB = 1 or 2 selects the third form, SB = 0 the fourth,
+    // SB = 3 the fourth with its level loops unrolled (msl 4-6)
     f.cp.SB = b->tG ? b->tSB : 0;
-    f.cp.variant = f.cp.SB ? 3 : 4;
+    f.cp.variant = (f.cp.SB == 1 || f.cp.SB == 2) ? 3 : (f.cp.SB == 3 ? 5 : 4);
     if (f.cp.G > 4) {
       set_error("batch: contraction shape G=%d is not available in batched form", f.cp.G);
       return -1;
@@ -719,7 +724,7 @@ void* wlg_batch_stream(wlg_batch* b) { return b ? (void*)b->st : nullptr; }
 
 int wlg_batch_set_contract_shape(wlg_batch* b, int G, int SB, int nCB, int block) {
   set_error("%s", "");
-  if (!b || G < 0 || G > 4 || SB < 0 || SB > 2 || nCB < 0 ||
+  if (!b || G < 0 || G > 4 || SB < 0 || SB > 3 || nCB < 0 ||
       (block != 0 && (block % 32 != 0 || block > 128))) {
     set_error("batch_set_contract_shape: bad shape");
     return -1;

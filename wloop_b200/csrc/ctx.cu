@@ -790,7 +790,7 @@ int wlg_reset_kernel_times(wlg_ctx* c) {
 
 int wlg_set_contract_tuning(wlg_ctx* c, int variant, int G, int SB, int nCB, int block) {
   CTX_BEGIN(c);
-  if (variant == 1 || variant < 0 || variant > 4 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
+  if (variant == 1 || variant < 0 || variant > 5 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
       nCB < 0 || (block != 0 && (block % 32 != 0 || block > 128)) ||
       (variant == 2 && G == 6 && SB == 2) || (variant >= 3 && G > 4)) {
     set_error("bad contraction tuning (variant %d, G %d, SB %d, nCB %d, block %d)", variant, G,
@@ -820,6 +820,45 @@ int wlg_set_contract_shape(wlg_ctx* c, int G, int nCB, int block) {
 void* wlg_stream(wlg_ctx* c) { return c ? (void*)c->st : nullptr; }
 
 long long wlg_launch_count(void) { return g_launches.load(); }
+
+int wlg_gauge_transform(wlg_ctx* c, uint64_t seed, double eps) {
+  CTX_BEGIN(c);
+  if (!(eps > 0.0)) {
+    set_error("gauge_transform: eps must be positive");
+    return -1;
+  }
+  if (ensure(c->apeB, dir_bytes(c))) return -1;
+  if (c->prec == WLG_FP64)
+    gauge_transform<double>(c->g, view4<double>(c->U.p, c->g.vol), (double2*)c->apeB.p, seed, eps,
+                            c->st);
+  else
+    gauge_transform<float>(c->g, view4<float>(c->U.p, c->g.vol), (float2*)c->apeB.p, seed, eps,
+                           c->st);
+  return finish("gauge_transform");
+}
+
+int wlg_shift_links(wlg_ctx* c, const int s[4]) {
+  CTX_BEGIN(c);
+  if (!s) {
+    set_error("shift_links: null shift");
+    return -1;
+  }
+  if (c->bc == 0 && s[0] % c->g.n[0] != 0) {
+    // the zero time links at x0 = N0-1 would move into the bulk
+    set_error("shift_links: open boundary conditions allow spatial shifts only");
+    return -1;
+  }
+  if (ensure(c->apeA, field_bytes(c, 4))) return -1;
+  const size_t fb = field_bytes(c, 4);
+  WLG_CUDA(cudaMemcpyAsync(c->apeA.p, c->U.p, fb, cudaMemcpyDeviceToDevice, c->st));
+  if (c->prec == WLG_FP64)
+    shift_links<double>(c->g, view4<double>(c->apeA.p, c->g.vol), view4<double>(c->U.p, c->g.vol),
+                        s, c->st);
+  else
+    shift_links<float>(c->g, view4<float>(c->apeA.p, c->g.vol), view4<float>(c->U.p, c->g.vol), s,
+                       c->st);
+  return finish("shift_links");
+}
 
 int wlg_snapshot(wlg_ctx* c) {
   CTX_BEGIN(c);

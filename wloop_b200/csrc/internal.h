@@ -93,9 +93,10 @@ enum { BATCH_HYP3 = 0, BATCH_HYP2, BATCH_HYP1, BATCH_APE, BATCH_HYP3D1, BATCH_HY
 template <class T>
 void line_step_batch(const LArgs<T>* A, const long long* pre, int n, long long total,
                      cudaStream_t st);
+// msl: level count shared by all lattices of the launch (0 if they differ)
 template <class T>
 void contract_batch(int G, int SB, const CArgs<T>* A, const long long* pre, int n, long long nblocks,
-                    int block, size_t smem, cudaStream_t st);
+                    int block, size_t smem, int msl, cudaStream_t st);
 template <class T> size_t contract3_smem(const ContractPlan& p, int msl);
 RArgs reduce_args(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mwlr, int r,
                   const double* partial, double* wl_mat);
@@ -116,6 +117,15 @@ void openqcd_to_soa(const Geo& g, const double* ud, const int* ipt, Links<T> U, 
 template <class T>
 void soa_to_openqcd(const Geo& g, Links<T> U, const int* ipt, double* ud, int mu0, int mu1,
                     cudaStream_t st);
+
+// ---- symmetry transformations (symm.cu) ------------------------------------
+// U_mu(x) <- g(x) U_mu(x) g(x+mu)^dag with g a synthetic SU(3) field keyed by
+// seed (written to G, one direction array); dst(x) = src(x - s), periodic.
+template <class T>
+void gauge_transform(const Geo& g, Links<T> U, typename V2<T>::t* G, uint64_t seed, double eps,
+                     cudaStream_t st);
+template <class T>
+void shift_links(const Geo& g, Links<T> src, Links<T> dst, const int s[4], cudaStream_t st);
 
 // ---- synthetic fields (gen_dev.cu) -----------------------------------------
 // Writes the synthetic link field of the given seed/eps straight into SoA.

@@ -9,10 +9,11 @@
 // (U0 at xs, U0' at xs+R k) is the same trace, Re tr[(ub um)^dag (ul ubR)],
 // with C carried in registers along T: 2 msl M + 36 msl^2 flops.  One thread
 // owns one column (xs,k) at one start slice x0 and G bottom levels; the
-// msl*G traces of each T are summed over the warp by a transposing shuffle
-// reduction and accumulated in a per-warp shared-memory row, so no atomics
-// and a fixed summation order.  Every stage also has a batched kernel that
-// covers many lattices in one launch (flattened work list, find_item).
+// msl*G traces of each T are summed over the warp (through shared memory in
+// the default fourth form, by shuffles in the earlier forms) and accumulated
+// in a per-warp shared-memory row, so no atomics and a fixed summation order.
+// Every stage also has a batched kernel that covers many lattices in one
+// launch (flattened work list, find_item).
 #include "internal.h"
 
 namespace wlg {
@@ -237,17 +238,26 @@ ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hin
   p.G = G;
   p.SB = (msl >= 2 && G <= 4 && !(fp64 && G >= 3)) ? 2 : 1;
   // fourth form (staged top lines, shared-memory reduction) unless G = 6,
-  // which only the second form has
-  p.variant = (G <= 4) ? 4 : 2;
+  // which only the second form has; in FP32 with its level loops unrolled
+  // (form 5; the unrolled FP64 kernel spills registers)
+  p.variant = (G <= 4) ? (fp64 ? 4 : 5) : 2;
   p.ngrp = (msl + G - 1) / G;
   // FP64 stages twice the bytes per thread: 64-thread blocks keep 3 blocks per SM
-  p.block = block_hint > 0 ? block_hint : ((fp64 && p.variant == 4) ? 64 : 128);
+  p.block = block_hint > 0 ? block_hint : ((fp64 && p.variant >= 4) ? 64 : 128);
   int ncol = 3 * g.vs;
   int nCB = nCB_hint;
   if (nCB <= 0) {
+    // At least 8 blocks per SM, and at most 4 column passes per block: the
+    // blocks of neighbouring x0 read the same lines one step apart, and they
+    // only share them through L2 while they stay in step.  Long column loops
+    // let them drift apart (at 32^3x64 with 77 passes per block the launch
+    // read its lines from DRAM 5-7 times over and ran 20-25 % slower).
     long long want = (long long)num_sms() * 8;
     long long base = (long long)g.n[0] * p.ngrp;
     nCB = (int)((want + base - 1) / base);
+    const int passes = 4;
+    const int lockstep = (ncol + passes * p.block - 1) / (passes * p.block);
+    if (nCB < lockstep) nCB = lockstep;
     int maxcb = (ncol + p.block - 1) / p.block;
     if (nCB > maxcb) nCB = maxcb;
     if (nCB < 1) nCB = 1;
@@ -510,16 +520,18 @@ static void launch_contract3_sb(const Geo& g, const ContractPlan& p, const typen
 // and accumulates it.  No shuffles, no dependent reduction chains, and no
 // extra shared memory: the rows reuse the stage of the current step.
 // ---------------------------------------------------------------------------
-template <class T, int G>
+template <class T, int G, int MSL>
 __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
   extern __shared__ double acc[];  // [nwarps][mwlt][G][msl] doubles, then the line stage
   constexpr int NQ = Chunks<T>::N;
+  constexpr int UNR = MSL > 0 ? MSL : 1;  // level loops unrolled when msl is a constant
   static_assert(G <= NQ, "one stage chunk per bottom level");
 
   const Geo& g = A.g;
   const typename V2<T>::t* __restrict__ u0 = A.u0;
   const typename V2<T>::t* __restrict__ lines = A.lines;
-  const int msl = A.msl, mwlt = A.mwlt, R = A.R, ngrp = A.ngrp, nCB = A.nCB;
+  const int msl = MSL > 0 ? MSL : A.msl;
+  const int mwlt = A.mwlt, R = A.R, ngrp = A.ngrp, nCB = A.nCB;
   double* __restrict__ partial = A.partial;
   const int N0 = g.n[0], vs = g.vs, vol = g.vol;
   int b = bid;
@@ -577,6 +589,7 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
       const int t1 = (t0 + 1 == N0) ? 0 : t0 + 1;  // x0+T mod N0: the top slice
       const int stop = t1 * vs + xs;
       __syncwarp();  // previous step's rows are read before the stage is refilled
+#pragma unroll UNR
       for (int s2 = 0; s2 < msl; s2++) {
         const typename V2<T>::t* src = lk + (size_t)s2 * lvl;
 #pragma unroll
@@ -594,7 +607,7 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
         ld(ub, u0, vol, t0 * vs + xsR);
       }
       cp_async_wait_all();
-#pragma unroll 1
+#pragma unroll UNR
       for (int s2 = 0; s2 < msl; s2++) {
         M3<T> l;
         ld_stage<T>(l, myslot + s2 * NQ * qstride, qstride);
@@ -632,24 +645,28 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
   }
 }
 
-template <class T, int G, int MINB>
+template <class T, int G, int MSL, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_contract4(CArgs<T> A) {
-  contract4_body<T, G>(A, blockIdx.x);
+  contract4_body<T, G, MSL>(A, blockIdx.x);
 }
 
-template <class T, int G, int MINB>
+template <class T, int G, int MSL, int MINB>
 __global__ void __launch_bounds__(128, MINB) kb_contract4(const CArgs<T>* __restrict__ A,
                                                           const long long* __restrict__ pre, int n) {
   const int c = find_item(pre, n, (long long)blockIdx.x);
-  contract4_body<T, G>(A[c], (int)(blockIdx.x - pre[c]));
+  contract4_body<T, G, MSL>(A[c], (int)(blockIdx.x - pre[c]));
 }
 
-template <class T, int G>
-static void launch_contract4(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
-                             const typename V2<T>::t* lines, int msl, int mwlt, int R,
-                             double* partial, cudaStream_t st) {
+// level counts with their own fully unrolled kernels (the usual 4-6); others
+// run the generic kernel (MSL = 0)
+static inline int msl_variant(int msl) { return (msl >= 4 && msl <= 6) ? msl : 0; }
+
+template <class T, int G, int MSL>
+static void launch_contract4_m(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
+                               const typename V2<T>::t* lines, int msl, int mwlt, int R,
+                               double* partial, cudaStream_t st) {
   constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
-  auto kern = k_contract4<T, G, MINB>;
+  auto kern = k_contract4<T, G, MSL, MINB>;
   size_t smem = contract3_smem<T>(p, msl);
   static size_t smem_set = 48 * 1024;
   if (smem > smem_set) {
@@ -670,11 +687,24 @@ static void launch_contract4(const Geo& g, const ContractPlan& p, const typename
   WLG_LAUNCH_CHECK("contract");
 }
 
+// unroll_msl: msl to unroll the level loops for, 0 for the generic kernel
 template <class T, int G>
-static void launch_contract4_batch(const CArgs<T>* A, const long long* pre, int n, long long nblocks,
-                                   int block, size_t smem, cudaStream_t st) {
+static void launch_contract4(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
+                             const typename V2<T>::t* lines, int msl, int unroll_msl, int mwlt,
+                             int R, double* partial, cudaStream_t st) {
+  switch (msl_variant(unroll_msl)) {
+    case 4: launch_contract4_m<T, G, 4>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 5: launch_contract4_m<T, G, 5>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 6: launch_contract4_m<T, G, 6>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    default: launch_contract4_m<T, G, 0>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+  }
+}
+
+template <class T, int G, int MSL>
+static void launch_contract4_batch_m(const CArgs<T>* A, const long long* pre, int n,
+                                     long long nblocks, int block, size_t smem, cudaStream_t st) {
   constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
-  auto kern = kb_contract4<T, G, MINB>;
+  auto kern = kb_contract4<T, G, MSL, MINB>;
   static size_t smem_set = 48 * 1024;
   if (smem > smem_set) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -684,16 +714,30 @@ static void launch_contract4_batch(const CArgs<T>* A, const long long* pre, int 
   WLG_LAUNCH_CHECK("contract_batch");
 }
 
+// msl: the level count shared by every lattice of the launch, or 0
+template <class T, int G>
+static void launch_contract4_batch(const CArgs<T>* A, const long long* pre, int n, long long nblocks,
+                                   int block, size_t smem, int msl, cudaStream_t st) {
+  switch (msl_variant(msl)) {
+    case 4: launch_contract4_batch_m<T, G, 4>(A, pre, n, nblocks, block, smem, st); break;
+    case 5: launch_contract4_batch_m<T, G, 5>(A, pre, n, nblocks, block, smem, st); break;
+    case 6: launch_contract4_batch_m<T, G, 6>(A, pre, n, nblocks, block, smem, st); break;
+    default: launch_contract4_batch_m<T, G, 0>(A, pre, n, nblocks, block, smem, st); break;
+  }
+}
+
 template <class T>
 void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
               const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
               cudaStream_t st) {
-  if (p.variant == 4) {
+  if (p.variant == 4 || p.variant == 5) {
+    // form 5: form 4 with the level loops unrolled for msl 4-6
+    const int m = p.variant == 5 ? msl : 0;
     switch (p.G) {
-      case 1: launch_contract4<T, 1>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
-      case 2: launch_contract4<T, 2>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
-      case 3: launch_contract4<T, 3>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
-      case 4: launch_contract4<T, 4>(g, p, u0, lines, msl, mwlt, R, partial, st); return;
+      case 1: launch_contract4<T, 1>(g, p, u0, lines, msl, m, mwlt, R, partial, st); return;
+      case 2: launch_contract4<T, 2>(g, p, u0, lines, msl, m, mwlt, R, partial, st); return;
+      case 3: launch_contract4<T, 3>(g, p, u0, lines, msl, m, mwlt, R, partial, st); return;
+      case 4: launch_contract4<T, 4>(g, p, u0, lines, msl, m, mwlt, R, partial, st); return;
       default: break;
     }
   }
@@ -809,14 +853,14 @@ static void launch_contract3_batch(const CArgs<T>* A, const long long* pre, int 
 
 template <class T>
 void contract_batch(int G, int SB, const CArgs<T>* A, const long long* pre, int n, long long nblocks,
-                    int block, size_t smem, cudaStream_t st) {
+                    int block, size_t smem, int msl, cudaStream_t st) {
   if (n <= 0 || nblocks <= 0) return;
   if (SB == 0) {  // fourth form (shared-memory reduction)
     switch (G) {
-      case 1: launch_contract4_batch<T, 1>(A, pre, n, nblocks, block, smem, st); return;
-      case 2: launch_contract4_batch<T, 2>(A, pre, n, nblocks, block, smem, st); return;
-      case 3: launch_contract4_batch<T, 3>(A, pre, n, nblocks, block, smem, st); return;
-      case 4: launch_contract4_batch<T, 4>(A, pre, n, nblocks, block, smem, st); return;
+      case 1: launch_contract4_batch<T, 1>(A, pre, n, nblocks, block, smem, msl, st); return;
+      case 2: launch_contract4_batch<T, 2>(A, pre, n, nblocks, block, smem, msl, st); return;
+      case 3: launch_contract4_batch<T, 3>(A, pre, n, nblocks, block, smem, msl, st); return;
+      case 4: launch_contract4_batch<T, 4>(A, pre, n, nblocks, block, smem, msl, st); return;
     }
   }
   if (SB == 2) {
@@ -854,9 +898,9 @@ template void line_step_batch<double>(const LArgs<double>*, const long long*, in
 template void line_step_batch<float>(const LArgs<float>*, const long long*, int, long long,
                                      cudaStream_t);
 template void contract_batch<double>(int, int, const CArgs<double>*, const long long*, int,
-                                     long long, int, size_t, cudaStream_t);
+                                     long long, int, size_t, int, cudaStream_t);
 template void contract_batch<float>(int, int, const CArgs<float>*, const long long*, int, long long,
-                                    int, size_t, cudaStream_t);
+                                    int, size_t, int, cudaStream_t);
 template size_t contract3_smem<double>(const ContractPlan&, int);
 template size_t contract3_smem<float>(const ContractPlan&, int);
 }  // namespace wlg
