@@ -293,3 +293,34 @@ def test_parameter_errors():
                   WloopParms(msl=1, nss=[0], mwlt=1, mwlr=1, op_smear=5)]:
             with pytest.raises(Exception):
                 c.wloop_sum(p)
+
+
+# every contraction form and shape the tuner or a caller may pick gives the
+# default's result up to summation order (including 32-thread blocks with an
+# odd number of per-warp row doubles, where the line stage must still start on
+# a 16-byte boundary)
+SHAPES = [  # (form, G, SB, nCB, block)
+    (2, 1, 1, 0, 64), (2, 3, 2, 0, 128), (3, 1, 2, 0, 64), (3, 3, 1, 0, 128), (3, 2, 2, 5, 96),
+    (4, 3, 0, 0, 32), (4, 1, 0, 7, 64), (4, 2, 0, 0, 128), (5, 3, 0, 0, 32), (5, 2, 0, 3, 64),
+    (5, 4, 0, 0, 128),
+]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", [1, 4])
+def test_contract_shapes(case, prec):
+    n, bc, p = CASES[case]
+    u = generate_links(n, bc, 300 + case, 0.25)
+    with Context(n, bc, prec) as c:
+        c.upload(u)
+        c.snapshot()
+        ref = c.measure(p)
+        scale = np.maximum(np.abs(ref), 1e-3)
+        for form, G, SB, ncb, block in SHAPES:
+            if G > p.msl:
+                continue
+            c.set_contract_tuning(form, G, SB, ncb, block)
+            c.restore()
+            got = c.measure(p)
+            tol = 1e-13 if prec == "fp64" else 1e-6
+            assert np.max(np.abs(got - ref) / scale) < tol, (form, G, SB, ncb, block)

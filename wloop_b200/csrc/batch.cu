@@ -294,7 +294,7 @@ template <class T> void build_ops(wlg_batch* b) {
         lu.push_back((long long)f.p.msl * 3 * f.g.vol);
         L = (const T2*)lines[c];
       }
-      CArgs<T> ca;
+      CArgs<T> ca{};
       ca.g = f.g;
       ca.u0 = (const T2*)base(f.U);
       ca.lines = L;
@@ -304,6 +304,8 @@ template <class T> void build_ops(wlg_batch* b) {
       ca.ngrp = f.cp.ngrp;
       ca.nCB = f.cp.nCB;
       ca.partial = (double*)(b->pbuf + f.partial);
+      ca.level = nullptr;  // the batch runs the line step as its own stage
+      ca.next = nullptr;
       Group* gp = nullptr;
       for (auto& gr : groups)
         if (gr.G == f.cp.G && gr.SB == f.cp.SB && gr.block == f.cp.block) gp = &gr;

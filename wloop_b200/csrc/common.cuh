@@ -124,6 +124,10 @@ template <class T> struct CArgs {
   const typename V2<T>::t* lines;  // [msl][3] spatial lines of length R
   int msl, mwlt, R, ngrp, nCB;
   double* partial;
+  // optional, fourth form only: next[sl][k](x) = lines[sl][k](x) * level[sl][k](x + R k),
+  // the lines of length R+1 (null: not computed)
+  const typename V2<T>::t* level;
+  typename V2<T>::t* next;
 };
 
 // Arguments of one partial-sum reduction (loops.cu): wl for spatial extent r

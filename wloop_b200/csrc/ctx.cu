@@ -58,7 +58,9 @@ struct wlg_ctx {
   int dev = 0, prec = WLG_FP64, bc = 3;
   Geo g;
   cudaStream_t st = nullptr;
-  DevBuf U, U0, bar, til, apeA, apeB, dl, levels, lines, partial, wl, plaq_part, plaq_out, staging, ipt;
+  DevBuf U, U0, bar, til, apeA, apeB, dl, levels, lines, lines2, partial, wl, plaq_part, plaq_out,
+      staging, ipt;
+  void* lines_at = nullptr;  // buffer holding the lines of length lines_len
   int cG = 0, cNCB = 0, cBlock = 0, cVariant = 0, cSB = 0;
   bool prof = false;
   std::map<std::string, ProfStat> stats;
@@ -359,21 +361,34 @@ static int do_loops(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
   if (ensure(c->partial, sizeof(double) * cp.partial_doubles) || ensure(c->wl, sizeof(double) * nwl))
     return -1;
   if (p->mwlr > 1 && ensure(c->lines, f3 * msl)) return -1;
+  // forms 4 and 5 compute the lines of the next R inside the contraction
+  // (ping-pong between two line buffers); other forms run the line step
+  const bool fuse = contract_fuses_lines(cp);
+  if (fuse && p->mwlr > 2 && ensure(c->lines2, f3 * msl)) return -1;
   c->lines_len = 0;
+  c->lines_at = nullptr;
   const T2* lev = (const T2*)c->levels.p;
   T2* lines = (T2*)c->lines.p;
+  T2* buf[2] = {(T2*)c->lines.p, (T2*)c->lines2.p};
+  const T2* L = lev;
   for (int r = 0; r < p->mwlr; r++) {
     const int R = r + 1;
-    const T2* L = lev;
-    if (R >= 2) {
+    if (!fuse && R >= 2) {
       ProfScope ps(c, "lines");
       line_step<T>(g, msl, R, lev, R == 2 ? lev : lines, lines, c->st);
       L = lines;
       c->lines_len = R;
+      c->lines_at = lines;
     }
+    T2* next = (fuse && R < p->mwlr) ? buf[r & 1] : nullptr;
     {
       ProfScope ps(c, "contract");
-      contract<T>(g, cp, U.p[0], L, msl, p->mwlt, R, (double*)c->partial.p, c->st);
+      contract<T>(g, cp, U.p[0], L, msl, p->mwlt, R, (double*)c->partial.p, lev, next, c->st);
+    }
+    if (next) {
+      L = next;
+      c->lines_len = R + 1;
+      c->lines_at = next;
     }
     {
       ProfScope ps(c, "reduce");
@@ -474,6 +489,9 @@ int wlg_free_scratch(wlg_ctx* c) {
   release(c->dl);
   release(c->levels);
   release(c->lines);
+  release(c->lines2);
+  c->lines_at = nullptr;
+  c->lines_len = 0;
   release(c->partial);
   release(c->staging);
   return 0;
@@ -484,7 +502,7 @@ int wlg_destroy(wlg_ctx* c) {
   cudaSetDevice(c->dev);
   cudaStreamSynchronize(c->st);
   harvest(c);
-  DevBuf* all[] = {&c->U, &c->U0, &c->bar, &c->til, &c->apeA, &c->apeB, &c->dl, &c->levels, &c->lines,
+  DevBuf* all[] = {&c->U, &c->U0, &c->bar, &c->til, &c->apeA, &c->apeB, &c->dl, &c->levels, &c->lines, &c->lines2,
                    &c->partial, &c->wl, &c->plaq_part, &c->plaq_out, &c->staging, &c->ipt};
   for (DevBuf* b : all) release(*b);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
@@ -666,11 +684,11 @@ int wlg_download_level(wlg_ctx* c, int sl, double* aos3) {
 int wlg_download_lines(wlg_ctx* c, int sl, double* aos3, int* length) {
   CTX_BEGIN(c);
   if (length) *length = c->lines_len;
-  if (!c->lines.p || c->lines_len < 2 || sl < 0 || sl >= c->last_msl) {
+  if (!c->lines_at || c->lines_len < 2 || sl < 0 || sl >= c->last_msl) {
     set_error("no spatial lines of level %d", sl);
     return -1;
   }
-  return download_spatial(c, (char*)c->lines.p + field_bytes(c, 3) * sl, aos3);
+  return download_spatial(c, (char*)c->lines_at + field_bytes(c, 3) * sl, aos3);
 }
 
 static int download_spatial(wlg_ctx* c, void* base, double* aos3) {

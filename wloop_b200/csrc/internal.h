@@ -75,10 +75,14 @@ struct ContractPlan {
 };
 ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hint, int nCB_hint,
                            int block_hint);
+// With next non-null (forms 4 and 5 only) the launch also writes the lines of
+// length R+1: next[sl][k](x) = lines[sl][k](x) level[sl][k](x + R k); next
+// must not alias lines or level.
 template <class T>
 void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
               const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
-              cudaStream_t st);
+              const typename V2<T>::t* level, typename V2<T>::t* next, cudaStream_t st);
+inline bool contract_fuses_lines(const ContractPlan& p) { return p.variant == 4 || p.variant == 5; }
 // Sums the partials and writes wl_mat[wl_idx(s1,s2,t,r,x0)] / norm.
 void contract_reduce(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mwlr, int r,
                      const double* partial, double* wl_mat, cudaStream_t st);

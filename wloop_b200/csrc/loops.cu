@@ -263,7 +263,8 @@ ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hin
     if (nCB < 1) nCB = 1;
   }
   p.nCB = nCB;
-  p.smem = (size_t)(p.block / 32) * mwlt * G * msl * sizeof(double);
+  // per-warp rows; rounded to 16 bytes, where the line stage starts
+  p.smem = (((size_t)(p.block / 32) * mwlt * G * msl + 1) & ~(size_t)1) * sizeof(double);
   p.partial_doubles = (size_t)g.n[0] * p.ngrp * nCB * mwlt * G * msl;
   return p;
 }
@@ -360,7 +361,8 @@ __device__ __forceinline__ void contract3_body(const CArgs<T>& A, int bid) {
   const int rowlen = mwlt * G * msl;
   double* wacc = acc + (size_t)warp * rowlen;
   // line stage: [msl][NQ][blockDim] 16-byte chunks; this thread's slot of chunk (s2,q)
-  char* stage = reinterpret_cast<char*>(acc + (size_t)nwarps * rowlen);
+  // 16-byte aligned for the 16-byte copies (an even number of doubles)
+  char* stage = reinterpret_cast<char*>(acc + (((size_t)nwarps * rowlen + 1) & ~(size_t)1));
   const int qstride = blockDim.x * 16;
   char* myslot = stage + threadIdx.x * 16;
   for (int i = lane; i < rowlen; i += 32) wacc[i] = 0.0;
@@ -485,7 +487,7 @@ static void launch_contract3(const Geo& g, const ContractPlan& p, const typename
     smem_set = smem;
   }
   int grid = g.n[0] * p.ngrp * p.nCB;
-  CArgs<T> A;
+  CArgs<T> A{};
   A.g = g;
   A.u0 = u0;
   A.lines = lines;
@@ -542,7 +544,8 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int rowlen = mwlt * G * msl;
   double* wacc = acc + (size_t)warp * rowlen;
-  char* stage = reinterpret_cast<char*>(acc + (size_t)nwarps * rowlen);
+  // 16-byte aligned for the 16-byte copies (an even number of doubles)
+  char* stage = reinterpret_cast<char*>(acc + (((size_t)nwarps * rowlen + 1) & ~(size_t)1));
   const int qstride = blockDim.x * 16;
   char* myslot = stage + threadIdx.x * 16;
   char* wchunks = stage + warp * 32 * 16;  // this warp's part of chunk (s2,q): + (s2*NQ+q)*qstride
@@ -580,6 +583,22 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
       int s1 = min(s1_0 + gi, msl - 1);
       ld(C[gi], lk + (size_t)s1 * lvl, vol, x0 * vs + xs);
       if (!active) zero(C[gi]);  // idle lanes contribute exact zeros
+    }
+    if (A.next) {
+      // the spatial line step of the next R (compute_uk_long, wloop.c:207-258)
+      // for this thread's own bottom lines: every (x0, column, level) has
+      // exactly one owner, and the product is line_step_item's
+      const size_t kof = (size_t)k * fstride;
+#pragma unroll
+      for (int gi = 0; gi < G; gi++) {
+        const int s1 = s1_0 + gi;
+        if (active && s1 < msl) {
+          M3<T> lv, nx;
+          ld(lv, A.level + kof + (size_t)s1 * lvl, vol, x0 * vs + xsR);
+          mul(nx, C[gi], lv);
+          st(A.next + kof + (size_t)s1 * lvl, vol, x0 * vs + xs, nx);
+        }
+      }
     }
     M3<T> ua, ub;
     ld(ua, u0, vol, x0 * vs + xs);
@@ -664,7 +683,8 @@ static inline int msl_variant(int msl) { return (msl >= 4 && msl <= 6) ? msl : 0
 template <class T, int G, int MSL>
 static void launch_contract4_m(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
                                const typename V2<T>::t* lines, int msl, int mwlt, int R,
-                               double* partial, cudaStream_t st) {
+                               double* partial, const typename V2<T>::t* level,
+                               typename V2<T>::t* next, cudaStream_t st) {
   constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
   auto kern = k_contract4<T, G, MSL, MINB>;
   size_t smem = contract3_smem<T>(p, msl);
@@ -673,7 +693,7 @@ static void launch_contract4_m(const Geo& g, const ContractPlan& p, const typena
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     smem_set = smem;
   }
-  CArgs<T> A;
+  CArgs<T> A{};
   A.g = g;
   A.u0 = u0;
   A.lines = lines;
@@ -683,6 +703,8 @@ static void launch_contract4_m(const Geo& g, const ContractPlan& p, const typena
   A.ngrp = p.ngrp;
   A.nCB = p.nCB;
   A.partial = partial;
+  A.level = level;
+  A.next = next;
   kern<<<g.n[0] * p.ngrp * p.nCB, p.block, smem, st>>>(A);
   WLG_LAUNCH_CHECK("contract");
 }
@@ -691,12 +713,13 @@ static void launch_contract4_m(const Geo& g, const ContractPlan& p, const typena
 template <class T, int G>
 static void launch_contract4(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
                              const typename V2<T>::t* lines, int msl, int unroll_msl, int mwlt,
-                             int R, double* partial, cudaStream_t st) {
+                             int R, double* partial, const typename V2<T>::t* level,
+                             typename V2<T>::t* next, cudaStream_t st) {
   switch (msl_variant(unroll_msl)) {
-    case 4: launch_contract4_m<T, G, 4>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
-    case 5: launch_contract4_m<T, G, 5>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
-    case 6: launch_contract4_m<T, G, 6>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
-    default: launch_contract4_m<T, G, 0>(g, p, u0, lines, msl, mwlt, R, partial, st); break;
+    case 4: launch_contract4_m<T, G, 4>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
+    case 5: launch_contract4_m<T, G, 5>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
+    case 6: launch_contract4_m<T, G, 6>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
+    default: launch_contract4_m<T, G, 0>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
   }
 }
 
@@ -729,15 +752,19 @@ static void launch_contract4_batch(const CArgs<T>* A, const long long* pre, int 
 template <class T>
 void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
               const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
-              cudaStream_t st) {
+              const typename V2<T>::t* level, typename V2<T>::t* next, cudaStream_t st) {
+  if (next && !contract_fuses_lines(p)) {
+    set_error("contract: this form does not compute the next lines");
+    return;
+  }
   if (p.variant == 4 || p.variant == 5) {
     // form 5: form 4 with the level loops unrolled for msl 4-6
     const int m = p.variant == 5 ? msl : 0;
     switch (p.G) {
-      case 1: launch_contract4<T, 1>(g, p, u0, lines, msl, m, mwlt, R, partial, st); return;
-      case 2: launch_contract4<T, 2>(g, p, u0, lines, msl, m, mwlt, R, partial, st); return;
-      case 3: launch_contract4<T, 3>(g, p, u0, lines, msl, m, mwlt, R, partial, st); return;
-      case 4: launch_contract4<T, 4>(g, p, u0, lines, msl, m, mwlt, R, partial, st); return;
+      case 1: launch_contract4<T, 1>(g, p, u0, lines, msl, m, mwlt, R, partial, level, next, st); return;
+      case 2: launch_contract4<T, 2>(g, p, u0, lines, msl, m, mwlt, R, partial, level, next, st); return;
+      case 3: launch_contract4<T, 3>(g, p, u0, lines, msl, m, mwlt, R, partial, level, next, st); return;
+      case 4: launch_contract4<T, 4>(g, p, u0, lines, msl, m, mwlt, R, partial, level, next, st); return;
       default: break;
     }
   }
@@ -886,9 +913,9 @@ template void line_step<double>(const Geo&, int, int, const double2*, const doub
 template void line_step<float>(const Geo&, int, int, const float2*, const float2*, float2*,
                                cudaStream_t);
 template void contract<double>(const Geo&, const ContractPlan&, const double2*, const double2*, int,
-                               int, int, double*, cudaStream_t);
+                               int, int, double*, const double2*, double2*, cudaStream_t);
 template void contract<float>(const Geo&, const ContractPlan&, const float2*, const float2*, int,
-                              int, int, double*, cudaStream_t);
+                              int, int, double*, const float2*, float2*, cudaStream_t);
 
 }  // namespace wlg
 
