@@ -369,18 +369,40 @@ __device__ __forceinline__ void project(M3<double>& u, int iter) {
     u.e[k].y *= d;
   }
   for (int it = 0; it < iter; it++) {
+    // X = 3/2 - U^dag U / 2 (projection.c:144-146).  U^dag U is Hermitian:
+    // its real diagonal and upper triangle are formed, the lower triangle is
+    // their conjugate (the full product gives the same numbers up to the
+    // rounding of an exactly vanishing diagonal imaginary part).
     M3<double> x, y;
-    mul_da(x, u, u);
 #pragma unroll
-    for (int k = 0; k < 9; k++) {
-      x.e[k].x *= -0.5;
-      x.e[k].y *= -0.5;
+    for (int i = 0; i < 3; i++) {
+      double dg = 0.0;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        dg = fma(u.e[3 * k + i].x, u.e[3 * k + i].x, dg);
+        dg = fma(u.e[3 * k + i].y, u.e[3 * k + i].y, dg);
+      }
+      x.e[4 * i].x = fma(-0.5, dg, 1.5);
+      x.e[4 * i].y = 0.0;
+#pragma unroll
+      for (int j = i + 1; j < 3; j++) {
+        double re = 0.0, im = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          re = fma(u.e[3 * k + i].x, u.e[3 * k + j].x, re);
+          re = fma(u.e[3 * k + i].y, u.e[3 * k + j].y, re);
+          im = fma(u.e[3 * k + i].x, u.e[3 * k + j].y, im);
+          im = fma(-u.e[3 * k + i].y, u.e[3 * k + j].x, im);
+        }
+        x.e[3 * i + j].x = -0.5 * re;
+        x.e[3 * i + j].y = -0.5 * im;
+        x.e[3 * j + i].x = -0.5 * re;
+        x.e[3 * j + i].y = 0.5 * im;
+      }
     }
-    x.e[0].x += 1.5;
-    x.e[4].x += 1.5;
-    x.e[8].x += 1.5;
     mul(y, u, x);
-    double zim = det_im(y) / -3.0;
+    // z = 1 - i Im det(Y) / 3 (projection.c:150-152)
+    double zim = det_im(y) * (-1.0 / 3.0);
 #pragma unroll
     for (int k = 0; k < 9; k++) {
       u.e[k].x = y.e[k].x - zim * y.e[k].y;

@@ -234,7 +234,12 @@ template <class T> __global__ void __launch_bounds__(128) k_hyp_l2(SArgs<T> A) {
 template <class T> __global__ void __launch_bounds__(128) k_hyp_l1(SArgs<T> A) {
   WLG_GRID_STRIDE((long long)A.nmu * A.g.vol) hyp_l1_item<T>(A, w);
 }
-template <class T> __global__ void __launch_bounds__(128) k_ape(SArgs<T> A) {
+// minimum resident blocks: FP32 fits 5 blocks of 128 threads per SM in 96
+// registers, FP64 3 blocks (the staples' latency needs the extra warps)
+template <class T> struct ApeMinBlocks { enum { v = sizeof(T) == 4 ? 5 : 3 }; };
+
+template <class T>
+__global__ void __launch_bounds__(128, ApeMinBlocks<T>::v) k_ape(SArgs<T> A) {
   WLG_GRID_STRIDE((long long)(4 - A.mu0) * A.g.vol) ape_item<T>(A, w);
 }
 template <class T> __global__ void __launch_bounds__(128) k_hyp3_l1(SArgs<T> A) {
