@@ -281,6 +281,19 @@ int wlg_dat_read(const char* path, long long rec, int* nc, double* wl_mat, int w
 int wlg_par_write_wloop(const char* path, const wlg_wloop_parms* p);
 int wlg_par_check_wloop(const char* path, long long offset, const wlg_wloop_parms* p);
 
+/* ---- gauge configurations in openQCD's exported format (host only) ---------
+ * What ms10 reads with import_cnfg (main/ms10.c:709-718; the format belongs
+ * to openQCD, which the reference does not include): 4 int32 extents, one
+ * double (the writer's average plaquette), then for every odd point in
+ * lexicographic order the 8 links U(x,0), U(x-0,0), ..., U(x,3), U(x-3,3) as
+ * su3_dble, little-endian.  links: [V][4][18] doubles, lexicographic sites.
+ * The plaquette is passed through as stored, not recomputed or checked.
+ * Errors return -1 with the message in wlg_cnfg_error(). */
+const char* wlg_cnfg_error(void);
+int wlg_cnfg_read_head(const char* path, int n[4], double* plaq);
+int wlg_cnfg_import(const char* path, const int n[4], double* links, double* plaq);
+int wlg_cnfg_export(const char* path, const int n[4], const double* links, double plaq);
+
 #ifdef __cplusplus
 }
 #endif

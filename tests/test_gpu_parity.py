@@ -303,11 +303,14 @@ SHAPES = [  # (form, G, SB, nCB, block)
     (2, 1, 1, 0, 64), (2, 3, 2, 0, 128), (3, 1, 2, 0, 64), (3, 3, 1, 0, 128), (3, 2, 2, 5, 96),
     (4, 3, 0, 0, 32), (4, 1, 0, 7, 64), (4, 2, 0, 0, 128), (5, 3, 0, 0, 32), (5, 2, 0, 3, 64),
     (5, 4, 0, 0, 128),
+    # bulk-copy staging (forms 6 and 7; on lattices whose time slices are not
+    # whole 32-site tiles they run as forms 5 and 4)
+    (6, 3, 0, 0, 128), (6, 2, 0, 5, 32), (7, 3, 0, 0, 64), (7, 1, 0, 0, 96), (6, 4, 0, 3, 64),
 ]
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-@pytest.mark.parametrize("case", [1, 4])
+@pytest.mark.parametrize("case", [0, 1, 4, 8])
 def test_contract_shapes(case, prec):
     n, bc, p = CASES[case]
     u = generate_links(n, bc, 300 + case, 0.25)

@@ -128,6 +128,10 @@ def _load():
         "wlg_dat_read": (i, [C.c_char_p, C.c_longlong, ip, dp, i]),
         "wlg_par_write_wloop": (i, [C.c_char_p, C.POINTER(WlgParms)]),
         "wlg_par_check_wloop": (i, [C.c_char_p, C.c_longlong, C.POINTER(WlgParms)]),
+        "wlg_cnfg_error": (C.c_char_p, []),
+        "wlg_cnfg_read_head": (i, [C.c_char_p, ip, dp]),
+        "wlg_cnfg_import": (i, [C.c_char_p, ip, dp, dp]),
+        "wlg_cnfg_export": (i, [C.c_char_p, ip, dp, d]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

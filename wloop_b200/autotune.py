@@ -53,8 +53,11 @@ def candidates(msl: int, fp64: bool, batched: bool) -> List[Shape]:
     for G in gs:
         if fp64 and G > 3:
             continue
-        # SB 0: fourth form (shared-memory reduction); 1, 2: third form
-        for SB in ((1,) if G == 6 else (0, 1, 2)):
+        # SB 0: the fourth-form family (shared-memory reduction; its best
+        # member for the precision); 1, 2: third form; batches also try SB 3,
+        # the fourth form with its level loops unrolled (msl 4-6)
+        sbs = (1,) if G == 6 else ((0, 1, 2, 3) if batched and 4 <= msl <= 6 else (0, 1, 2))
+        for SB in sbs:
             for block in ((64,) if fp64 else (64, 128)):
                 out.append((G, SB, block, 0))
     return out
@@ -133,8 +136,9 @@ def tune_batch(batch, reps: int = 1, use_cache: bool = True) -> Shape:
 
 
 def _form(G: int, SB: int) -> int:
-    """kernel form of a shape: 2 for G = 6, 4 for SB = 0, else 3"""
-    return 2 if G > 4 else (4 if SB == 0 else 3)
+    """kernel form of a context shape: 2 for G = 6, 3 for SB = 1 or 2, and
+    for SB = 0 the library's default fourth-form member (0 = automatic)"""
+    return 2 if G > 4 else (0 if SB == 0 else 3)
 
 
 def _as_batch(shape: Shape):

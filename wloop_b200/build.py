@@ -32,7 +32,7 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin", HO
            "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"] + ARCH
 
 CU_SOURCES = ["ctx.cu", "smear.cu", "loops.cu", "layout.cu", "gen_dev.cu", "batch.cu", "noalloc.cu", "symm.cu"]
-CXX_SOURCES = ["gen_host.cpp", "legacy.cpp", "serve.cpp", "datfile.cpp"]
+CXX_SOURCES = ["gen_host.cpp", "legacy.cpp", "serve.cpp", "datfile.cpp", "cnfg.cpp"]
 
 
 def _sources_present():

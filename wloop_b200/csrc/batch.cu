@@ -7,8 +7,10 @@
 //
 // Memory: one arena per batch.  Per lattice: the gauge field, its snapshot,
 // and one region that holds the HYP scratch while HYP runs and afterwards the
-// APE ping-pong buffers, the level store and the spatial lines (HYP has
-// finished for every lattice before the first sweep writes there).
+// APE ping-pong buffers, the level store and two spatial-line buffers (HYP
+// has finished for every lattice before the first sweep writes there).  The
+// contraction forms 4-7 write the next R's lines themselves, alternating
+// between the two line buffers; the third form runs a line-step stage.
 #include <string.h>
 
 #include <algorithm>
@@ -184,7 +186,7 @@ template <class T> void build_ops(wlg_batch* b) {
   // per lattice: cur = spatial links of U; sweep i of level sl writes the
   // level slot on its last sweep, else the ping-pong buffer not holding cur
   std::vector<Links<T>> cur(n), A(n), B(n);
-  std::vector<char*> levels(n), lines(n), dl(n);
+  std::vector<char*> levels(n), lines(n), lines2(n), dl(n);
   int maxmsl = 0, maxr = 0;
   for (int c = 0; c < n; c++) {
     const Cfg& f = b->cfg[c];
@@ -195,6 +197,7 @@ template <class T> void build_ops(wlg_batch* b) {
     levels[c] = r + 6 * f.D * es;
     lines[c] = r + (6 + 3 * (size_t)f.p.msl) * f.D * es;
     dl[c] = r + (6 + 6 * (size_t)f.p.msl) * f.D * es;
+    lines2[c] = r + (12 + 6 * (size_t)f.p.msl) * f.D * es;
     cur[c] = lview<T>(base(f.U) + f.D * es, f.D, 3, 1);
     maxmsl = std::max(maxmsl, f.p.msl);
     maxr = std::max(maxr, f.p.mwlr);
@@ -282,7 +285,10 @@ template <class T> void build_ops(wlg_batch* b) {
       if (r >= f.p.mwlr) continue;
       const T2* lev = (const T2*)levels[c];
       const T2* L = lev;
-      if (R >= 2) {
+      const bool fuse = contract_fuses_lines(f.cp);
+      T2* buf[2] = {(T2*)lines[c], (T2*)lines2[c]};
+      if (fuse && R >= 2) L = buf[(R - 2) & 1];
+      if (!fuse && R >= 2) {
         LArgs<T> x;
         x.g = f.g;
         x.msl = f.p.msl;
@@ -304,8 +310,8 @@ template <class T> void build_ops(wlg_batch* b) {
       ca.ngrp = f.cp.ngrp;
       ca.nCB = f.cp.nCB;
       ca.partial = (double*)(b->pbuf + f.partial);
-      ca.level = nullptr;  // the batch runs the line step as its own stage
-      ca.next = nullptr;
+      ca.level = lev;
+      ca.next = (fuse && R < f.p.mwlr) ? buf[(R - 1) & 1] : nullptr;
       Group* gp = nullptr;
       for (auto& gr : groups)
         if (gr.G == f.cp.G && gr.SB == f.cp.SB && gr.block == f.cp.block) gp = &gr;
@@ -438,7 +444,9 @@ void layout(wlg_batch* b) {
     f.U0 = off;
     off = align256(off + 4 * f.D * es);
     f.region = off;
-    size_t rdirs = std::max<size_t>(24, 12 + 6 * (size_t)f.p.msl);
+    // APE ping-pong 6 + levels 3 msl + lines 3 msl + spatial-HYP scratch 6 +
+    // second lines 3 msl, or the HYP scratch (24), whichever is larger
+    size_t rdirs = std::max<size_t>(24, 12 + 9 * (size_t)f.p.msl);
     off = align256(off + rdirs * f.D * es);
     f.nwl = (size_t)f.p.msl * f.p.msl * f.p.mwlt * f.p.mwlr * f.g.n[0];
     f.wl = off;

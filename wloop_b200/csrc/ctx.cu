@@ -72,6 +72,7 @@ struct wlg_ctx {
   std::vector<cudaEvent_t> evpool;
   int last_msl = 0;
   int lines_len = 0;
+  int used_variant = 0;  // contraction form of the last measurement
 };
 
 static int ensure(DevBuf& b, size_t bytes) {
@@ -357,6 +358,7 @@ static int do_loops(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
   ContractPlan cp = contract_plan(g, msl, p->mwlt, c->prec == WLG_FP64, c->cG, c->cNCB, c->cBlock);
   if (c->cVariant) cp.variant = c->cVariant;
   if (c->cSB) cp.SB = c->cSB;
+  c->used_variant = cp.variant;
   size_t nwl = (size_t)msl * msl * p->mwlt * p->mwlr * g.n[0];
   if (ensure(c->partial, sizeof(double) * cp.partial_doubles) || ensure(c->wl, sizeof(double) * nwl))
     return -1;
@@ -405,6 +407,10 @@ template <class T>
 static int do_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, double* plaq) {
   if (do_smear<T>(c, p, plaq) || do_loops<T>(c, p, wl_mat)) return -1;
   WLG_CUDA(cudaStreamSynchronize(c->st));
+  if (c->used_variant >= 6 && contract_stage_failed() != 0) {
+    set_error("wloop_sum: the contraction's staged-line copies did not arrive in time");
+    return -1;
+  }
   return finish("wloop_sum");
 }
 
@@ -808,7 +814,7 @@ int wlg_reset_kernel_times(wlg_ctx* c) {
 
 int wlg_set_contract_tuning(wlg_ctx* c, int variant, int G, int SB, int nCB, int block) {
   CTX_BEGIN(c);
-  if (variant == 1 || variant < 0 || variant > 5 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
+  if (variant == 1 || variant < 0 || variant > 7 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
       nCB < 0 || (block != 0 && (block % 32 != 0 || block > 128)) ||
       (variant == 2 && G == 6 && SB == 2) || (variant >= 3 && G > 4)) {
     set_error("bad contraction tuning (variant %d, G %d, SB %d, nCB %d, block %d)", variant, G,

@@ -82,7 +82,12 @@ template <class T>
 void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
               const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
               const typename V2<T>::t* level, typename V2<T>::t* next, cudaStream_t st);
-inline bool contract_fuses_lines(const ContractPlan& p) { return p.variant == 4 || p.variant == 5; }
+inline bool contract_fuses_lines(const ContractPlan& p) { return p.variant >= 4 && p.variant <= 7; }
+// the bulk-staged forms need time slices of whole 32-site tiles
+inline bool contract_can_bulk(const Geo& g) { return g.vs % 32 == 0; }
+// 1 if a bulk-staged contraction gave up waiting for its copies since the
+// last call (the flag is cleared), 0 if not, -1 if the flag cannot be read
+int contract_stage_failed();
 // Sums the partials and writes wl_mat[wl_idx(s1,s2,t,r,x0)] / norm.
 void contract_reduce(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mwlr, int r,
                      const double* partial, double* wl_mat, cudaStream_t st);

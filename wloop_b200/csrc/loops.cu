@@ -238,9 +238,10 @@ ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hin
   p.G = G;
   p.SB = (msl >= 2 && G <= 4 && !(fp64 && G >= 3)) ? 2 : 1;
   // fourth form (staged top lines, shared-memory reduction) unless G = 6,
-  // which only the second form has; in FP32 with its level loops unrolled
-  // (form 5; the unrolled FP64 kernel spills registers)
-  p.variant = (G <= 4) ? (fp64 ? 4 : 5) : 2;
+  // which only the second form has: in FP32 with its level loops unrolled
+  // (form 5; the unrolled FP64 kernel spills registers), in FP64 with the top
+  // lines staged by bulk copies (form 7; 5 % faster there, 2 % slower in FP32)
+  p.variant = (G <= 4) ? (fp64 ? 7 : 5) : 2;
   p.ngrp = (msl + G - 1) / G;
   // FP64 stages twice the bytes per thread: 64-thread blocks keep 3 blocks per SM
   p.block = block_hint > 0 ? block_hint : ((fp64 && p.variant >= 4) ? 64 : 128);
@@ -314,6 +315,58 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// ---- bulk (TMA) copies of whole 32-site tiles into shared memory ----------
+// One-dimensional cp.async.bulk from this GPU's global memory into this
+// CTA's shared memory, completing on an mbarrier (no multicast, no tensor
+// map).  Every wait is bounded: a wait that runs out sets g_stage_timeout,
+// which the host reads after the measurement.
+__device__ int g_stage_timeout;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+// at most 2^20 polls; false if the phase did not complete
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase) {
+  for (unsigned it = 0; it < (1u << 20); it++)
+    if (mbar_try_wait(bar, phase)) return true;
+  return false;
+}
+// orders this thread's earlier shared-memory accesses before later
+// async-proxy (bulk copy) writes to the same memory
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+// dst, src and bytes multiples of 16
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
 
 // 16-byte chunk q of link s in a tiled direction array (common.cuh layout)
 template <class T> __device__ __forceinline__ const char* chunk_ptr(const typename V2<T>::t* base, int s, int q);
@@ -457,8 +510,9 @@ __device__ __forceinline__ void contract3_body(const CArgs<T>& A, int bid) {
   }
 }
 
+// rows, the line stage, and one mbarrier per warp (bulk-staged forms)
 template <class T> size_t contract3_smem(const ContractPlan& p, int msl) {
-  return p.smem + (size_t)msl * Chunks<T>::N * p.block * 16;
+  return p.smem + (size_t)msl * Chunks<T>::N * p.block * 16 + (size_t)(p.block / 32) * 8;
 }
 
 template <class T, int G, int SB, int MINB>
@@ -522,11 +576,17 @@ static void launch_contract3_sb(const Geo& g, const ContractPlan& p, const typen
 // and accumulates it.  No shuffles, no dependent reduction chains, and no
 // extra shared memory: the rows reuse the stage of the current step.
 // ---------------------------------------------------------------------------
-template <class T, int G, int MSL>
+// BULK: the msl top-line tiles of a warp's 32 columns arrive as msl bulk
+// copies of one tile each (one lane per level) on a per-warp mbarrier,
+// instead of 16-byte cp.async per thread and chunk.  Needs 32-aligned column
+// ranges inside one direction: N1 N2 N3 a multiple of 32 (the launcher
+// checks), column blocks rounded to 32 columns (below).
+template <class T, int G, int MSL, bool BULK>
 __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
-  extern __shared__ double acc[];  // [nwarps][mwlt][G][msl] doubles, then the line stage
+  extern __shared__ double acc[];  // [nwarps][mwlt][G][msl] doubles, the line stage, mbarriers
   constexpr int NQ = Chunks<T>::N;
   constexpr int UNR = MSL > 0 ? MSL : 1;  // level loops unrolled when msl is a constant
+  constexpr unsigned TILE_BYTES = NQ * 32 * 16;  // one direction tile of 32 links
   static_assert(G <= NQ, "one stage chunk per bottom level");
 
   const Geo& g = A.g;
@@ -546,15 +606,28 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
   double* wacc = acc + (size_t)warp * rowlen;
   // 16-byte aligned for the 16-byte copies (an even number of doubles)
   char* stage = reinterpret_cast<char*>(acc + (((size_t)nwarps * rowlen + 1) & ~(size_t)1));
-  const int qstride = blockDim.x * 16;
-  char* myslot = stage + threadIdx.x * 16;
-  char* wchunks = stage + warp * 32 * 16;  // this warp's part of chunk (s2,q): + (s2*NQ+q)*qstride
+  // the warp's stage: chunk (s2, q) of its 32 lanes at wchunks + (s2*NQ + q)*512,
+  // lane l's 16 bytes at + 16 l (the layout of a tile in global memory)
+  constexpr int qstride = 512;
+  char* wchunks = stage + (size_t)warp * msl * NQ * 512;
+  char* myslot = wchunks + lane * 16;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(stage + (size_t)nwarps * msl * NQ * 512) + warp;
+  unsigned phase = 0;
+  bool stage_ok = true;
   for (int i = lane; i < rowlen; i += 32) wacc[i] = 0.0;
+  if (BULK) {
+    if (lane == 0) {
+      mbar_init(bar, 1);
+      mbar_init_fence();
+    }
+  }
   __syncwarp();
 
   const int s1_0 = grp * G;
   const int ncol = 3 * vs;
-  const int per = (ncol + nCB - 1) / nCB;
+  // whole 32-column tiles per warp (needed by the bulk copies; kept for both
+  // staging paths so that they split the columns, and sum, identically)
+  const int per = (((ncol + nCB - 1) / nCB) + 31) & ~31;
   const int c_begin = cb * per;
   const int c_end = min(ncol, c_begin + per);
   const size_t fstride = link_elems<T>(vol);
@@ -607,15 +680,30 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
     for (int tt = 1; tt <= mwlt; tt++) {
       const int t1 = (t0 + 1 == N0) ? 0 : t0 + 1;  // x0+T mod N0: the top slice
       const int stop = t1 * vs + xs;
-      __syncwarp();  // previous step's rows are read before the stage is refilled
+      if (BULK) {
+        // every lane's reads and writes of the stage come before the copies
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (stage_ok) {
+          if (lane == 0) mbar_expect_tx(bar, (unsigned)msl * TILE_BYTES);
+          __syncwarp();
+          if (lane < msl) {
+            // the warp's 32 columns are one tile: site stop - lane of lane 0
+            const typename V2<T>::t* src = lk + (size_t)lane * lvl + (size_t)(stop >> 5) * Tile<T>::TS;
+            bulk_g2s(wchunks + (size_t)lane * NQ * 512, src, TILE_BYTES, bar);
+          }
+        }
+      } else {
+        __syncwarp();  // previous step's rows are read before the stage is refilled
 #pragma unroll UNR
-      for (int s2 = 0; s2 < msl; s2++) {
-        const typename V2<T>::t* src = lk + (size_t)s2 * lvl;
+        for (int s2 = 0; s2 < msl; s2++) {
+          const typename V2<T>::t* src = lk + (size_t)s2 * lvl;
 #pragma unroll
-        for (int q = 0; q < NQ; q++)
-          cp_async16(myslot + (s2 * NQ + q) * qstride, chunk_ptr<T>(src, stop, q));
+          for (int q = 0; q < NQ; q++)
+            cp_async16(myslot + (s2 * NQ + q) * qstride, chunk_ptr<T>(src, stop, q));
+        }
+        cp_async_commit();
       }
-      cp_async_commit();
 #pragma unroll
       for (int gi = 0; gi < G; gi++) lmul_dag_inplace(C[gi], ua);
 #pragma unroll
@@ -625,7 +713,21 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
         ld(ua, u0, vol, t0 * vs + xs);
         ld(ub, u0, vol, t0 * vs + xsR);
       }
-      cp_async_wait_all();
+      if (BULK) {
+        if (stage_ok) {
+          const bool done = mbar_wait_bounded(bar, phase);
+          if (__all_sync(0xffffffffu, done)) {
+            phase ^= 1u;
+          } else {
+            // the copies did not arrive: flag it, stop staging, finish with
+            // what is in the stage (the host discards the result)
+            stage_ok = false;
+            if (lane == 0) atomicExch(&g_stage_timeout, 1);
+          }
+        }
+      } else {
+        cp_async_wait_all();
+      }
 #pragma unroll UNR
       for (int s2 = 0; s2 < msl; s2++) {
         M3<T> l;
@@ -655,6 +757,7 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
       }
     }
   }
+  if (BULK && !stage_ok) mbar_wait_bounded(bar, phase);  // copies still in flight, bounded
   __syncthreads();
   double* out = partial + ((size_t)(x0 * ngrp + grp) * nCB + cb) * rowlen;
   for (int i = threadIdx.x; i < rowlen; i += blockDim.x) {
@@ -664,29 +767,29 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
   }
 }
 
-template <class T, int G, int MSL, int MINB>
+template <class T, int G, int MSL, int MINB, bool BULK>
 __global__ void __launch_bounds__(128, MINB) k_contract4(CArgs<T> A) {
-  contract4_body<T, G, MSL>(A, blockIdx.x);
+  contract4_body<T, G, MSL, BULK>(A, blockIdx.x);
 }
 
 template <class T, int G, int MSL, int MINB>
 __global__ void __launch_bounds__(128, MINB) kb_contract4(const CArgs<T>* __restrict__ A,
                                                           const long long* __restrict__ pre, int n) {
   const int c = find_item(pre, n, (long long)blockIdx.x);
-  contract4_body<T, G, MSL>(A[c], (int)(blockIdx.x - pre[c]));
+  contract4_body<T, G, MSL, false>(A[c], (int)(blockIdx.x - pre[c]));
 }
 
 // level counts with their own fully unrolled kernels (the usual 4-6); others
 // run the generic kernel (MSL = 0)
 static inline int msl_variant(int msl) { return (msl >= 4 && msl <= 6) ? msl : 0; }
 
-template <class T, int G, int MSL>
+template <class T, int G, int MSL, bool BULK>
 static void launch_contract4_m(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
                                const typename V2<T>::t* lines, int msl, int mwlt, int R,
                                double* partial, const typename V2<T>::t* level,
                                typename V2<T>::t* next, cudaStream_t st) {
   constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
-  auto kern = k_contract4<T, G, MSL, MINB>;
+  auto kern = k_contract4<T, G, MSL, MINB, BULK>;
   size_t smem = contract3_smem<T>(p, msl);
   static size_t smem_set = 48 * 1024;
   if (smem > smem_set) {
@@ -710,17 +813,28 @@ static void launch_contract4_m(const Geo& g, const ContractPlan& p, const typena
 }
 
 // unroll_msl: msl to unroll the level loops for, 0 for the generic kernel
+template <class T, int G, bool BULK>
+static void launch_contract4_b(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
+                               const typename V2<T>::t* lines, int msl, int unroll_msl, int mwlt,
+                               int R, double* partial, const typename V2<T>::t* level,
+                               typename V2<T>::t* next, cudaStream_t st) {
+  switch (msl_variant(unroll_msl)) {
+    case 4: launch_contract4_m<T, G, 4, BULK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
+    case 5: launch_contract4_m<T, G, 5, BULK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
+    case 6: launch_contract4_m<T, G, 6, BULK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
+    default: launch_contract4_m<T, G, 0, BULK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
+  }
+}
+
 template <class T, int G>
 static void launch_contract4(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
-                             const typename V2<T>::t* lines, int msl, int unroll_msl, int mwlt,
-                             int R, double* partial, const typename V2<T>::t* level,
+                             const typename V2<T>::t* lines, int msl, int unroll_msl, bool bulk,
+                             int mwlt, int R, double* partial, const typename V2<T>::t* level,
                              typename V2<T>::t* next, cudaStream_t st) {
-  switch (msl_variant(unroll_msl)) {
-    case 4: launch_contract4_m<T, G, 4>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
-    case 5: launch_contract4_m<T, G, 5>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
-    case 6: launch_contract4_m<T, G, 6>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
-    default: launch_contract4_m<T, G, 0>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
-  }
+  if (bulk)
+    launch_contract4_b<T, G, true>(g, p, u0, lines, msl, unroll_msl, mwlt, R, partial, level, next, st);
+  else
+    launch_contract4_b<T, G, false>(g, p, u0, lines, msl, unroll_msl, mwlt, R, partial, level, next, st);
 }
 
 template <class T, int G, int MSL>
@@ -757,14 +871,17 @@ void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
     set_error("contract: this form does not compute the next lines");
     return;
   }
-  if (p.variant == 4 || p.variant == 5) {
-    // form 5: form 4 with the level loops unrolled for msl 4-6
-    const int m = p.variant == 5 ? msl : 0;
+  if (p.variant >= 4 && p.variant <= 7) {
+    // form 5: form 4 with the level loops unrolled for msl 4-6; forms 6 / 7:
+    // forms 5 / 4 with the top lines staged by bulk copies, where a time
+    // slice is whole 32-site tiles (else they run as forms 5 / 4)
+    const int m = (p.variant == 5 || p.variant == 6) ? msl : 0;
+    const bool bulk = (p.variant >= 6) && contract_can_bulk(g);
     switch (p.G) {
-      case 1: launch_contract4<T, 1>(g, p, u0, lines, msl, m, mwlt, R, partial, level, next, st); return;
-      case 2: launch_contract4<T, 2>(g, p, u0, lines, msl, m, mwlt, R, partial, level, next, st); return;
-      case 3: launch_contract4<T, 3>(g, p, u0, lines, msl, m, mwlt, R, partial, level, next, st); return;
-      case 4: launch_contract4<T, 4>(g, p, u0, lines, msl, m, mwlt, R, partial, level, next, st); return;
+      case 1: launch_contract4<T, 1>(g, p, u0, lines, msl, m, bulk, mwlt, R, partial, level, next, st); return;
+      case 2: launch_contract4<T, 2>(g, p, u0, lines, msl, m, bulk, mwlt, R, partial, level, next, st); return;
+      case 3: launch_contract4<T, 3>(g, p, u0, lines, msl, m, bulk, mwlt, R, partial, level, next, st); return;
+      case 4: launch_contract4<T, 4>(g, p, u0, lines, msl, m, bulk, mwlt, R, partial, level, next, st); return;
       default: break;
     }
   }
@@ -912,6 +1029,19 @@ template void line_step<double>(const Geo&, int, int, const double2*, const doub
                                 cudaStream_t);
 template void line_step<float>(const Geo&, int, int, const float2*, const float2*, float2*,
                                cudaStream_t);
+int contract_stage_failed() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_stage_timeout, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  if (v) {
+    const int zero = 0;
+    cudaMemcpyToSymbol(g_stage_timeout, &zero, sizeof(int));
+  }
+  return v;
+}
+
 template void contract<double>(const Geo&, const ContractPlan&, const double2*, const double2*, int,
                                int, int, double*, const double2*, double2*, cudaStream_t);
 template void contract<float>(const Geo&, const ContractPlan&, const float2*, const float2*, int,

@@ -14,9 +14,9 @@ replicas: rank r measures every world-th configuration into its own file
 written.  No device data crosses ranks.
 
 Configurations come from a callable nc -> host field (complex128, shape
-(V, 4, 3, 3), su3_dble layout) or, without one, are synthetic fields
-generated on the device with seed nc.  Reading openQCD's exported
-configuration files belongs to openQCD and is not part of this module.
+(V, 4, 3, 3), su3_dble layout) -- `cnfg_source` reads ms10's exported files
+<cnfg_dir>/<name>n<nc> -- or, without one, are synthetic fields generated on
+the device with seed nc.
 """
 from __future__ import annotations
 
@@ -119,6 +119,50 @@ def write_par(path: str, p: WloopParms) -> None:
 def check_par(path: str, p: WloopParms, offset: int = 0) -> None:
     cp = p.to_c()
     _check(lib.wlg_par_check_wloop(_b(path), offset, C.byref(cp)), "check_wloop_parms")
+
+
+# ---------------------------------------------------------------------------
+# configurations in openQCD's exported format
+# ---------------------------------------------------------------------------
+def _cnfg_check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise WlgError(f"{what}: {lib.wlg_cnfg_error().decode(errors='replace')}")
+
+
+def cnfg_head(path: str) -> Tuple[Tuple[int, int, int, int], float]:
+    """(lattice extents, stored average plaquette) of an exported file."""
+    n = (C.c_int * 4)()
+    plaq = C.c_double()
+    _cnfg_check(lib.wlg_cnfg_read_head(_b(path), n, C.byref(plaq)), "import_cnfg")
+    return tuple(n), plaq.value
+
+
+def import_cnfg(path: str, n=None) -> np.ndarray:
+    """The field of an exported configuration as complex128 (V, 4, 3, 3),
+    lexicographic sites (the layout Context.upload takes)."""
+    if n is None:
+        n, _ = cnfg_head(path)
+    vol = int(np.prod(n))
+    u = np.empty((vol, 4, 3, 3), dtype=np.complex128)
+    _cnfg_check(lib.wlg_cnfg_import(_b(path), (C.c_int * 4)(*n), dptr(u.view(np.float64)), None),
+                "import_cnfg")
+    return u
+
+
+def export_cnfg(path: str, u: np.ndarray, n, plaq: float) -> None:
+    """Writes u (V, 4, 3, 3) in the exported format with the given plaquette
+    value in the head."""
+    u = np.ascontiguousarray(u, dtype=np.complex128)
+    _cnfg_check(lib.wlg_cnfg_export(_b(path), (C.c_int * 4)(*n), dptr(u.view(np.float64)),
+                                    float(plaq)), "export_cnfg")
+
+
+def cnfg_source(cnfg_dir: str, name: str, n) -> Callable[[int], np.ndarray]:
+    """nc -> field of <cnfg_dir>/<name>n<nc>, ms10's exported-file naming
+    (main/ms10.c:716)."""
+    def source(nc: int) -> np.ndarray:
+        return import_cnfg(os.path.join(cnfg_dir, f"{name}n{nc}"), tuple(n))
+    return source
 
 
 # ---------------------------------------------------------------------------
@@ -229,6 +273,9 @@ def main(argv=None) -> int:
     ap.add_argument("--step", type=int, default=1)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--eps", type=float, default=0.2)
+    ap.add_argument("--cnfg-dir", default=None,
+                    help="read <cnfg-dir>/<name>n<nc> in openQCD's exported format instead of "
+                         "generating synthetic fields")
     ap.add_argument("--msl", type=int, required=True)
     ap.add_argument("--nss", type=int, nargs="+", required=True)
     ap.add_argument("--mwlt", type=int, required=True)
@@ -245,7 +292,8 @@ def main(argv=None) -> int:
                    a.proj_iter)
     r = Run(a.name, n, a.bc, p, a.first, a.last, a.step, a.precision, a.eps)
     with Replicas() as rep:
-        res = run(r, a.out, rep, log=print if rep.rank == 0 else None)
+        src = cnfg_source(a.cnfg_dir, a.name, n) if a.cnfg_dir else None
+        res = run(r, a.out, rep, source=src, log=print if rep.rank == 0 else None)
     if res.get("merged"):
         print(f"{res['records']} records in {res['merged']}")
     return 0
