@@ -74,6 +74,15 @@ int wlg_free_scratch(wlg_ctx* ctx);
 
 /* ---- gauge field transfers ---------------------------------------------- */
 int wlg_upload_links(wlg_ctx* ctx, const double* aos);
+/* Pipelined upload: wlg_prefetch_links starts the host-to-device copy of the
+ * next field (same layout as wlg_upload_links) on the context's copy stream
+ * and returns at once, so the copy overlaps a measurement in progress;
+ * wlg_upload_prefetched makes it the context's gauge field (ordered after
+ * the copy on the context's stream).  The host buffer must stay unchanged
+ * until the copy is done (pinned memory makes it asynchronous).  One
+ * prefetch at a time. */
+int wlg_prefetch_links(wlg_ctx* ctx, const double* aos);
+int wlg_upload_prefetched(wlg_ctx* ctx);
 int wlg_download_links(wlg_ctx* ctx, double* aos);
 int wlg_upload_openqcd(wlg_ctx* ctx, const double* ud, const int* ipt);
 int wlg_download_openqcd(wlg_ctx* ctx, double* ud, const int* ipt);

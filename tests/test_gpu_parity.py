@@ -327,3 +327,28 @@ def test_contract_shapes(case, prec):
             got = c.measure(p)
             tol = 1e-13 if prec == "fp64" else 1e-6
             assert np.max(np.abs(got - ref) / scale) < tol, (form, G, SB, ncb, block)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_prefetched_upload(prec):
+    """The pipelined upload (copy on the copy stream, transposition on the
+    context's stream) gives the field an ordinary upload gives, also while a
+    measurement is running, and refuses misuse."""
+    n, bc, p = CASES[1]
+    u1 = generate_links(n, bc, 41, 0.25)
+    u2 = generate_links(n, bc, 42, 0.25)
+    with Context(n, bc, prec) as c:
+        c.upload(u2)
+        ref2 = c.measure(p)
+        c.upload(u1)
+        ref1 = c.measure(p)
+        with pytest.raises(Exception, match="no field was prefetched"):
+            c.upload_prefetched()
+        c.prefetch(u2)
+        with pytest.raises(Exception, match="has not been uploaded"):
+            c.prefetch(u1)
+        c.upload_prefetched()
+        c.prefetch(u1)          # overlaps the next measurement
+        assert np.array_equal(c.measure(p), ref2)
+        c.upload_prefetched()
+        assert np.array_equal(c.measure(p), ref1)

@@ -68,6 +68,8 @@ def _load():
         "wlg_free_scratch": (i, [vp]),
         "wlg_upload_links": (i, [vp, dp]),
         "wlg_download_links": (i, [vp, dp]),
+        "wlg_prefetch_links": (i, [vp, dp]),
+        "wlg_upload_prefetched": (i, [vp]),
         "wlg_upload_openqcd": (i, [vp, dp, ip]),
         "wlg_download_openqcd": (i, [vp, dp, ip]),
         "wlg_generate": (i, [vp, u64, d]),

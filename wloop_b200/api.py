@@ -135,6 +135,18 @@ class Context:
         assert u.size == self.vol * 36
         check(lib.wlg_upload_links(self._h, dptr(u.view(np.float64))), "upload")
 
+    def prefetch(self, u: np.ndarray) -> None:
+        """Starts copying the next field to the device while the current
+        measurement runs; `upload_prefetched` makes it the gauge field.  u
+        must stay alive and unchanged until then (pinned memory for overlap)."""
+        assert u.flags.c_contiguous and u.dtype == np.complex128 and u.size == self.vol * 36
+        self._prefetch_ref = u
+        check(lib.wlg_prefetch_links(self._h, dptr(u.view(np.float64))), "prefetch")
+
+    def upload_prefetched(self) -> None:
+        check(lib.wlg_upload_prefetched(self._h), "upload_prefetched")
+        self._prefetch_ref = None
+
     def download(self) -> np.ndarray:
         u = np.empty((self.vol, 4, 3, 3), dtype=np.complex128)
         check(lib.wlg_download_links(self._h, dptr(u.view(np.float64))), "download")

@@ -61,6 +61,11 @@ struct wlg_ctx {
   DevBuf U, U0, bar, til, apeA, apeB, dl, levels, lines, lines2, partial, wl, plaq_part, plaq_out,
       staging, ipt;
   void* lines_at = nullptr;  // buffer holding the lines of length lines_len
+  // prefetch: the next field's host-to-device copy on its own stream
+  DevBuf prefetch_buf;
+  cudaStream_t cst = nullptr;
+  cudaEvent_t copied = nullptr, consumed = nullptr;
+  bool prefetched = false;
   int cG = 0, cNCB = 0, cBlock = 0, cVariant = 0, cSB = 0;
   bool prof = false;
   std::map<std::string, ProfStat> stats;
@@ -488,6 +493,8 @@ int wlg_create(const int n[4], int bc, int precision, int device, wlg_ctx** out)
 int wlg_free_scratch(wlg_ctx* c) {
   CTX_BEGIN(c);
   WLG_CUDA(cudaStreamSynchronize(c->st));
+  if (c->cst) WLG_CUDA(cudaStreamSynchronize(c->cst));
+  if (!c->prefetched) release(c->prefetch_buf);
   release(c->bar);
   release(c->til);
   release(c->apeA);
@@ -507,11 +514,18 @@ int wlg_destroy(wlg_ctx* c) {
   if (!c) return 0;
   cudaSetDevice(c->dev);
   cudaStreamSynchronize(c->st);
+  if (c->cst) cudaStreamSynchronize(c->cst);
   harvest(c);
   DevBuf* all[] = {&c->U, &c->U0, &c->bar, &c->til, &c->apeA, &c->apeB, &c->dl, &c->levels, &c->lines, &c->lines2,
-                   &c->partial, &c->wl, &c->plaq_part, &c->plaq_out, &c->staging, &c->ipt};
+                   &c->partial, &c->wl, &c->plaq_part, &c->plaq_out, &c->staging, &c->ipt,
+                   &c->prefetch_buf};
   for (DevBuf* b : all) release(*b);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
+  if (c->cst) {
+    cudaEventDestroy(c->copied);
+    cudaEventDestroy(c->consumed);
+    cudaStreamDestroy(c->cst);
+  }
   cudaStreamDestroy(c->st);
   delete c;
   return 0;
@@ -534,6 +548,57 @@ int wlg_upload_links(wlg_ctx* c, const double* aos) {
     aos_to_soa<float>(c->g, (const double*)c->staging.p, view4<float>(c->U.p, c->g.vol), 0, 4, c->st);
   WLG_CUDA(cudaStreamSynchronize(c->st));
   return finish("upload_links");
+}
+
+// The host-to-device copy of the next field on a copy stream, so that it
+// overlaps the measurement running on the context's stream.
+int wlg_prefetch_links(wlg_ctx* c, const double* aos) {
+  CTX_BEGIN(c);
+  if (!aos) {
+    set_error("prefetch_links: null field");
+    return -1;
+  }
+  const size_t bytes = (size_t)4 * 144 * c->g.vol;
+  if (!c->cst) {
+    if (cudaStreamCreateWithFlags(&c->cst, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->copied, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->consumed, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("prefetch_links: stream or event creation failed");
+      return -1;
+    }
+    WLG_CUDA(cudaEventRecord(c->consumed, c->st));
+  }
+  if (c->prefetched) {
+    set_error("prefetch_links: the previous prefetched field has not been uploaded");
+    return -1;
+  }
+  if (c->prefetch_buf.cap < bytes) {
+    WLG_CUDA(cudaStreamSynchronize(c->cst));
+    if (ensure(c->prefetch_buf, bytes)) return -1;
+  }
+  // the buffer's previous contents have been transposed into U
+  WLG_CUDA(cudaStreamWaitEvent(c->cst, c->consumed, 0));
+  WLG_CUDA(cudaMemcpyAsync(c->prefetch_buf.p, aos, bytes, cudaMemcpyHostToDevice, c->cst));
+  WLG_CUDA(cudaEventRecord(c->copied, c->cst));
+  c->prefetched = true;
+  return finish("prefetch_links");
+}
+
+int wlg_upload_prefetched(wlg_ctx* c) {
+  CTX_BEGIN(c);
+  if (!c->prefetched) {
+    set_error("upload_prefetched: no field was prefetched");
+    return -1;
+  }
+  WLG_CUDA(cudaStreamWaitEvent(c->st, c->copied, 0));
+  if (c->prec == WLG_FP64)
+    aos_to_soa<double>(c->g, (const double*)c->prefetch_buf.p, view4<double>(c->U.p, c->g.vol), 0, 4, c->st);
+  else
+    aos_to_soa<float>(c->g, (const double*)c->prefetch_buf.p, view4<float>(c->U.p, c->g.vol), 0, 4, c->st);
+  WLG_CUDA(cudaEventRecord(c->consumed, c->st));
+  c->prefetched = false;
+  return finish("upload_prefetched");
 }
 
 int wlg_download_links(wlg_ctx* c, double* aos) {
