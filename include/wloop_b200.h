@@ -266,6 +266,11 @@ int wlg_restore(wlg_ctx* ctx);
  * unchanged by the first and move to W(x0 - s0) under the second. */
 int wlg_gauge_transform(wlg_ctx* ctx, uint64_t seed, double eps);
 int wlg_shift_links(wlg_ctx* ctx, const int s[4]);
+/* Self-test of the contraction's bounded wait for its staged lines: a
+ * one-warp kernel waits for a copy that never comes, with the given limit
+ * (0 < limit_s <= 10); *timed_out = 1 and the elapsed time show that the wait
+ * ends by itself and reports instead of hanging. */
+int wlg_selftest_wait(int device, double limit_s, int* timed_out, double* elapsed_s);
 /* Achievable vector FMA throughput of the device in TFLOP/s (2 flops per
  * FMA), FP64 or FP32 (precision WLG_FP64 / WLG_MIXED). */
 int wlg_peak_flops(int precision, int device, double* tflops);

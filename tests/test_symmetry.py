@@ -154,3 +154,21 @@ def test_full_size_invariances(prec):
     ts = tol_shift(p, vol) if prec == "fp64" else max(tol_shift(p, vol), 1e-6)
     assert rel_dev(wg, w0) < tg
     assert rel_dev(ws, np.roll(w0, block)) < ts
+
+
+def test_bounded_wait_ends():
+    """The bounded wait of the bulk-staged contraction, on a barrier that no
+    copy completes: it ends at its limit and reports, and the device stays
+    usable for the next measurement."""
+    import ctypes as C
+    from wloop_b200._native import lib
+    out, el = C.c_int(-1), C.c_double(-1.0)
+    assert lib.wlg_selftest_wait(0, 0.2, C.byref(out), C.byref(el)) == 0
+    assert out.value == 1
+    assert 0.2 <= el.value < 2.0
+    n, bc, p = CASES[0]
+    with Context(n, bc, "fp64") as c:
+        c.generate(3, 0.2)
+        c.set_contract_tuning(7, 3, 0, 0, 64)
+        w1 = c.measure(p)
+    assert np.all(np.isfinite(w1))

@@ -96,6 +96,7 @@ def _load():
         "wlg_shift_links": (i, [vp, ip]),
         "wlg_restore": (i, [vp]),
         "wlg_peak_flops": (i, [i, i, dp]),
+        "wlg_selftest_wait": (i, [i, d, ip, dp]),
         "wlg_batch_create": (i, [i, ip, ip, C.POINTER(WlgParms), i, i, C.POINTER(vp)]),
         "wlg_batch_destroy": (i, [vp]),
         "wlg_batch_size": (i, [vp]),

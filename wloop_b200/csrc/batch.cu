@@ -233,7 +233,7 @@ template <class T> void build_ops(wlg_batch* b) {
           x.a = f.p.alpha_ape;
           x.mu0 = 1;
           ape.push_back(x);
-          u3.push_back(3LL * f.g.vol);
+          u3.push_back(ape_items(f.g.vol, 1));
         } else {
           // spatial HYP: level 1 from cur into dl, copy cur -> dst, level 2 in place on dst
           x.U = cur[c];

@@ -949,6 +949,24 @@ int wlg_shift_links(wlg_ctx* c, const int s[4]) {
   return finish("shift_links");
 }
 
+int wlg_selftest_wait(int device, double limit_s, int* timed_out, double* elapsed_s) {
+  set_error("%s", "");
+  if (!timed_out || !elapsed_s || !(limit_s > 0.0) || limit_s > 10.0) {
+    set_error("selftest_wait: bad arguments (limit 0 < s <= 10)");
+    return -1;
+  }
+  if (device < 0 || device >= wlg_device_count() || cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("selftest_wait: no device %d", device);
+    return -1;
+  }
+  if (wait_selftest(limit_s, timed_out, elapsed_s)) {
+    set_error("selftest_wait: %s", cudaGetErrorString(cudaGetLastError()));
+    return -1;
+  }
+  return 0;
+}
+
 int wlg_snapshot(wlg_ctx* c) {
   CTX_BEGIN(c);
   if (ensure(c->U0, field_bytes(c, 4))) return -1;

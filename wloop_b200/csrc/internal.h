@@ -27,6 +27,11 @@ void hyp_level2(const Geo& g, Links<T> U, const typename V2<T>::t* vbar, typenam
 template <class T>
 void hyp_level1(const Geo& g, Links<T> U, const typename V2<T>::t* vtil, double a1, int proj,
                 int iter, int mu0, int mu1, int bc, cudaStream_t st);
+// Work items of one APE sweep over directions [mu0,4): the volume rounded up
+// to whole 32-site tiles, per direction (items are ordered tile-major).
+__host__ __device__ inline long long ape_items(int vol, int mu0) {
+  return (long long)(4 - mu0) * ((vol + 31) & ~31);
+}
 // One APE sweep dst = P[src + alpha * staples] over directions [mu0,4)
 // (ape_links.c:147-272).  dst must not alias src.
 template <class T>
@@ -88,6 +93,8 @@ inline bool contract_can_bulk(const Geo& g) { return g.vs % 32 == 0; }
 // 1 if a bulk-staged contraction gave up waiting for its copies since the
 // last call (the flag is cleared), 0 if not, -1 if the flag cannot be read
 int contract_stage_failed();
+// runs the bounded-wait self-test on the current device (0 or -1)
+int wait_selftest(double limit_s, int* timed_out, double* elapsed_s);
 // Sums the partials and writes wl_mat[wl_idx(s1,s2,t,r,x0)] / norm.
 void contract_reduce(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mwlr, int r,
                      const double* partial, double* wl_mat, cudaStream_t st);

@@ -348,11 +348,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
       : "memory");
   return ok != 0;
 }
-// at most 2^20 polls; false if the phase did not complete
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase) {
-  for (unsigned it = 0; it < (1u << 20); it++)
-    if (mbar_try_wait(bar, phase)) return true;
-  return false;
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;\n" : "=l"(t));
+  return t;
+}
+// waits at most limit_ns of wall time (the global nanosecond timer bounds it,
+// whatever each try_wait's own suspension); false if the phase did not complete
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase,
+                                                  uint64_t limit_ns = 2000000000ull) {
+  if (mbar_try_wait(bar, phase)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_wait(bar, phase))
+    if (global_ns() - t0 > limit_ns) return false;
+  return true;
 }
 // orders this thread's earlier shared-memory accesses before later
 // async-proxy (bulk copy) writes to the same memory
@@ -1029,6 +1038,48 @@ template void line_step<double>(const Geo&, int, int, const double2*, const doub
                                 cudaStream_t);
 template void line_step<float>(const Geo&, int, int, const float2*, const float2*, float2*,
                                cudaStream_t);
+// Self-test of the bounded wait: one warp arms an mbarrier for bytes that no
+// copy ever delivers and waits with the given limit, as the contraction
+// waits for its staged lines; the outcome goes to out[0] (1: the wait ran
+// out) and out[1] (elapsed ns).  Nothing faults or hangs: the wait ends at
+// the limit and the barrier is left in shared memory that the block frees.
+__global__ void k_wait_selftest(uint64_t limit_ns, unsigned long long* out) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+  if (threadIdx.x == 0) mbar_expect_tx(&bar, 512);  // no copy follows
+  __syncwarp();
+  const uint64_t t0 = global_ns();
+  const bool done = mbar_wait_bounded(&bar, 0, limit_ns);
+  const uint64_t t1 = global_ns();
+  if (!__all_sync(0xffffffffu, done) && threadIdx.x == 0) {
+    out[0] = 1;
+    out[1] = t1 - t0;
+  } else if (threadIdx.x == 0) {
+    out[0] = 0;
+    out[1] = t1 - t0;
+  }
+}
+
+int wait_selftest(double limit_s, int* timed_out, double* elapsed_s) {
+  unsigned long long* d = nullptr;
+  unsigned long long h[2] = {0, 0};
+  if (cudaMalloc(&d, sizeof(h)) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  k_wait_selftest<<<1, 32>>>((uint64_t)(limit_s * 1e9), d);
+  cudaError_t e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return -1;
+  *timed_out = (int)h[0];
+  *elapsed_s = h[1] * 1e-9;
+  return 0;
+}
+
 int contract_stage_failed() {
   int v = 0;
   if (cudaMemcpyFromSymbol(&v, g_stage_timeout, sizeof(int)) != cudaSuccess) {

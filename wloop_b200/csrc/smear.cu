@@ -134,10 +134,18 @@ template <class T> __device__ __forceinline__ void hyp_l1_item(const SArgs<T>& A
 }
 
 // One APE sweep (ape_links_all, ape_links.c:217-272):
-//   D(x,mu) = P[U(x,mu) + alpha * sum_{eta != mu} S_eta(U)];  w in [0, (4-mu0) V)
+//   D(x,mu) = P[U(x,mu) + alpha * sum_{eta != mu} S_eta(U)];
+// w in [0, ape_items(vol, mu0)), tile-major: the 4-mu0 directions of one
+// 32-site tile are consecutive warps, so the links their staples share are
+// re-read from L2 instead of once per direction sweep over the whole field.
 template <class T> __device__ __forceinline__ void ape_item(const SArgs<T>& A, long long w) {
   const Geo& g = A.g;
-  int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+  const int nmu = 4 - A.mu0;
+  const long long tile = w / (32 * nmu);
+  const int rem = (int)(w - tile * 32 * nmu);
+  const int q = rem >> 5;
+  const int s = (int)(tile * 32) + (rem & 31);
+  if (s >= g.vol) return;  // the last tile of a lattice whose volume is not a multiple of 32
   int mu = A.mu0 + q;
   int x[4];
   coords(g, s, x);
@@ -240,7 +248,7 @@ template <class T> struct ApeMinBlocks { enum { v = sizeof(T) == 4 ? 5 : 3 }; };
 
 template <class T>
 __global__ void __launch_bounds__(128, ApeMinBlocks<T>::v) k_ape(SArgs<T> A) {
-  WLG_GRID_STRIDE((long long)(4 - A.mu0) * A.g.vol) ape_item<T>(A, w);
+  WLG_GRID_STRIDE(ape_items(A.g.vol, A.mu0)) ape_item<T>(A, w);
 }
 template <class T> __global__ void __launch_bounds__(128) k_hyp3_l1(SArgs<T> A) {
   WLG_GRID_STRIDE(6LL * A.g.vol) hyp3_l1_item<T>(A, w);
@@ -459,7 +467,7 @@ void ape_sweep(const Geo& g, Links<T> src, Links<T> dst, double alpha, int proj,
   A.proj = proj;
   A.iter = iter;
   A.mu0 = mu0;
-  k_ape<T><<<grid_for((long long)(4 - mu0) * g.vol, 128), 128, 0, st>>>(A);
+  k_ape<T><<<grid_for(ape_items(g.vol, mu0), 128), 128, 0, st>>>(A);
   WLG_LAUNCH_CHECK("ape_sweep");
 }
 template <class T>
