@@ -174,8 +174,8 @@ template <class T> void build_ops(wlg_batch* b) {
       x.a = 1.0 - f.p.alpha_action[0];
       x.b = f.p.alpha_action[0] / 6.0;
       a1.push_back(x);
-      u12.push_back(12LL * f.g.vol);
-      u4.push_back(4LL * f.g.vol);
+      u12.push_back(tile_items(f.g.vol, 12));
+      u4.push_back(tile_items(f.g.vol, 4));
     }
     push_smear(BATCH_HYP3, a3, u12);
     push_smear(BATCH_HYP2, a2, u12);

@@ -27,11 +27,22 @@ void hyp_level2(const Geo& g, Links<T> U, const typename V2<T>::t* vbar, typenam
 template <class T>
 void hyp_level1(const Geo& g, Links<T> U, const typename V2<T>::t* vtil, double a1, int proj,
                 int iter, int mu0, int mu1, int bc, cudaStream_t st);
-// Work items of one APE sweep over directions [mu0,4): the volume rounded up
-// to whole 32-site tiles, per direction (items are ordered tile-major).
-__host__ __device__ inline long long ape_items(int vol, int mu0) {
-  return (long long)(4 - mu0) * ((vol + 31) & ~31);
+// Work items of a smearing pass with nq outputs per site, ordered
+// tile-major: item w is output q of site s with the nq outputs of one 32-site
+// tile in consecutive warps, so the neighbour links their staples share are
+// re-read from L2 rather than once per output over the whole field.  The
+// volume is rounded up to whole tiles; items past the volume do nothing.
+__host__ __device__ inline long long tile_items(int vol, int nq) {
+  return (long long)nq * ((vol + 31) & ~31);
 }
+__host__ __device__ inline void tile_item(long long w, int nq, int& q, int& s) {
+  const long long tile = w / (32 * nq);
+  const int rem = (int)(w - tile * 32 * nq);
+  q = rem >> 5;
+  s = (int)(tile * 32) + (rem & 31);
+}
+// APE sweep over directions [mu0,4)
+__host__ __device__ inline long long ape_items(int vol, int mu0) { return tile_items(vol, 4 - mu0); }
 // One APE sweep dst = P[src + alpha * staples] over directions [mu0,4)
 // (ape_links.c:147-272).  dst must not alias src.
 template <class T>

@@ -63,10 +63,12 @@ __device__ __forceinline__ void lcomb_project(M3<double>& v, double a, const M3<
 // ---------------------------------------------------------------------------
 
 // HYP level with alpha3 (decorated_links1, hyp_links.c:320-373):
-//   vbar[p(mu,eta)](x,mu) = P[(1-a3) U + a3/2 * S_eta(U)];  w in [0, 12V)
+//   vbar[p(mu,eta)](x,mu) = P[(1-a3) U + a3/2 * S_eta(U)];  w in [0, tile_items(V, 12))
 template <class T> __device__ __forceinline__ void hyp_l3_item(const SArgs<T>& A, long long w) {
   const Geo& g = A.g;
-  int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+  int q, s;
+  tile_item(w, 12, q, s);
+  if (s >= g.vol) return;
   int mu = q / 3, eta = (mu + 1 + q % 3) & 3;
   int x[4];
   coords(g, s, x);
@@ -83,10 +85,12 @@ template <class T> __device__ __forceinline__ void hyp_l3_item(const SArgs<T>& A
 
 // HYP level with alpha2 (decorated_links2, hyp_links.c:244-317):
 //   vtil[p(mu,nu)](x,mu) = P[(1-a2) U + a2/4 * sum_{rho != mu,nu} S_rho]
-//   rho-links from vbar[p(mu,nu)], mu-links from vbar[p(nu,rho)];  w in [0, 12V)
+//   rho-links from vbar[p(mu,nu)], mu-links from vbar[p(nu,rho)];  w in [0, tile_items(V, 12))
 template <class T> __device__ __forceinline__ void hyp_l2_item(const SArgs<T>& A, long long w) {
   const Geo& g = A.g;
-  int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+  int q, s;
+  tile_item(w, 12, q, s);
+  if (s >= g.vol) return;
   int mu = q / 3, nu = (mu + 1 + q % 3) & 3;
   int x[4];
   coords(g, s, x);
@@ -109,10 +113,12 @@ template <class T> __device__ __forceinline__ void hyp_l2_item(const SArgs<T>& A
 
 // HYP level with alpha1 (decorated_links3, hyp_links.c:194-241) and the copy
 // back into the gauge field (:432-447), in place: each item reads only its
-// own U(x,mu) for the linear combination.  w in [0, nmu V)
+// own U(x,mu) for the linear combination.  w in [0, tile_items(V, nmu))
 template <class T> __device__ __forceinline__ void hyp_l1_item(const SArgs<T>& A, long long w) {
   const Geo& g = A.g;
-  int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
+  int q, s;
+  tile_item(w, A.nmu, q, s);
+  if (s >= g.vol) return;
   int mu = A.mu0 + q;
   int x[4];
   coords(g, s, x);
@@ -140,11 +146,8 @@ template <class T> __device__ __forceinline__ void hyp_l1_item(const SArgs<T>& A
 // re-read from L2 instead of once per direction sweep over the whole field.
 template <class T> __device__ __forceinline__ void ape_item(const SArgs<T>& A, long long w) {
   const Geo& g = A.g;
-  const int nmu = 4 - A.mu0;
-  const long long tile = w / (32 * nmu);
-  const int rem = (int)(w - tile * 32 * nmu);
-  const int q = rem >> 5;
-  const int s = (int)(tile * 32) + (rem & 31);
+  int q, s;
+  tile_item(w, 4 - A.mu0, q, s);
   if (s >= g.vol) return;  // the last tile of a lattice whose volume is not a multiple of 32
   int mu = A.mu0 + q;
   int x[4];
@@ -234,13 +237,13 @@ __global__ void __launch_bounds__(128) kb_smear(const SArgs<T>* __restrict__ A,
 }
 
 template <class T> __global__ void __launch_bounds__(128) k_hyp_l3(SArgs<T> A) {
-  WLG_GRID_STRIDE(12LL * A.g.vol) hyp_l3_item<T>(A, w);
+  WLG_GRID_STRIDE(tile_items(A.g.vol, 12)) hyp_l3_item<T>(A, w);
 }
 template <class T> __global__ void __launch_bounds__(128) k_hyp_l2(SArgs<T> A) {
-  WLG_GRID_STRIDE(12LL * A.g.vol) hyp_l2_item<T>(A, w);
+  WLG_GRID_STRIDE(tile_items(A.g.vol, 12)) hyp_l2_item<T>(A, w);
 }
 template <class T> __global__ void __launch_bounds__(128) k_hyp_l1(SArgs<T> A) {
-  WLG_GRID_STRIDE((long long)A.nmu * A.g.vol) hyp_l1_item<T>(A, w);
+  WLG_GRID_STRIDE(tile_items(A.g.vol, A.nmu)) hyp_l1_item<T>(A, w);
 }
 // minimum resident blocks: FP32 fits 5 blocks of 128 threads per SM in 96
 // registers, FP64 3 blocks (the staples' latency needs the extra warps)
@@ -422,7 +425,7 @@ void hyp_level3(const Geo& g, Links<T> U, typename V2<T>::t* vbar, double a3, in
   A.b = a3 / 2.0;
   A.proj = proj;
   A.iter = iter;
-  k_hyp_l3<T><<<grid_for(12LL * g.vol, 128), 128, 0, st>>>(A);
+  k_hyp_l3<T><<<grid_for(tile_items(g.vol, 12), 128), 128, 0, st>>>(A);
   WLG_LAUNCH_CHECK("hyp_level3");
 }
 template <class T>
@@ -436,7 +439,7 @@ void hyp_level2(const Geo& g, Links<T> U, const typename V2<T>::t* vbar, typenam
   A.b = a2 / 4.0;
   A.proj = proj;
   A.iter = iter;
-  k_hyp_l2<T><<<grid_for(12LL * g.vol, 128), 128, 0, st>>>(A);
+  k_hyp_l2<T><<<grid_for(tile_items(g.vol, 12), 128), 128, 0, st>>>(A);
   WLG_LAUNCH_CHECK("hyp_level2");
 }
 template <class T>
@@ -454,7 +457,7 @@ void hyp_level1(const Geo& g, Links<T> U, const typename V2<T>::t* vtil, double 
   A.mu0 = mu0;
   A.nmu = nmu;
   A.bc = bc;
-  k_hyp_l1<T><<<grid_for((long long)nmu * g.vol, 128), 128, 0, st>>>(A);
+  k_hyp_l1<T><<<grid_for(tile_items(g.vol, nmu), 128), 128, 0, st>>>(A);
   WLG_LAUNCH_CHECK("hyp_level1");
 }
 template <class T>
