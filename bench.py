@@ -307,15 +307,28 @@ def run_ours(args, rank, world, local):
     if os.path.exists(peaks_file):
         with open(peaks_file) as f:
             hbm = json.load(f).get("hbm_gbs")
+    # algorithmic bytes of one launch: its lines of length R and temporal links
+    # ((3 msl + 1) V links) plus the fused line step's level links in and new
+    # lines out (2 x 3 msl V, for 15 of the 16 launches)
+    link_b = 72 if args.precision == "mixed" else 144
+    vol = w.volume
+    bytes_per_launch = link_b * vol * ((3 * p.msl + 1) + 6 * p.msl * (p.mwlr - 1) / p.mwlr)
+    hbm_ach = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
     roof = {"kernel": "k_contract4 (loop contraction with the fused spatial line step)",
             "bound": "fp32" if args.precision == "mixed" else "fp64",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "peak_source": "vector FMA probe measured in this run (wlg_peak_flops); "
-                           "MEASURED_PEAKS.json has no CUDA-core peak",
+            "peak_source": "vector FMA probe measured in this run (wlg_peak_flops; of measured); "
+                           "the kernel is bound by CUDA-core FMA throughput, not by HBM or "
+                           "tensor cores (3x3 complex products have no tensor-core form), "
+                           "and MEASURED_PEAKS.json has no CUDA-core peak",
             "flops_per_launch": flops_per_launch, "ms_per_launch": per_launch_ms,
-            "traffic": traffic}
-    if traffic and hbm:
-        roof["hbm_frac_of_measured"] = traffic / (per_launch_ms * 1e-3) / 1e9 / hbm
+            "traffic": traffic,
+            "hbm": {"achieved": hbm_ach, "peak": hbm, "unit": "GB/s",
+                    "frac": (hbm_ach / hbm) if hbm else None,
+                    "algorithmic_bytes_per_launch": bytes_per_launch,
+                    "traffic_frac": (traffic / (per_launch_ms * 1e-3) / 1e9 / hbm)
+                    if (traffic and hbm) else None,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}}
     total_ms = sum(v[0] for v in kt.values())
     shares = {k: round(v[0] / total_ms, 4) for k, v in kt.items() if total_ms > 0}
 

@@ -172,6 +172,10 @@ int wlg_batch_result(wlg_batch* b, int i, double* wl_mat);
 /* device time of the last run and kernels per run */
 int wlg_batch_stats(wlg_batch* b, double* last_ms, int* kernels_per_run);
 void* wlg_batch_stream(wlg_batch* b);
+/* Device memory of batches comes from a stream-ordered pool per device that
+ * keeps what batches free for the next batch; this is how much of it is idle
+ * (free for batches, not visible to cudaMemGetInfo). */
+long long wlg_batch_pool_idle_bytes(int device);
 /* contraction shape for the whole batch (0 = automatic); G <= 4; SB selects
  * the form: 1 or 2 the third (SB levels per reduction), 0 the fourth, 3 the
  * fourth with its level loops unrolled (msl 4-6) */

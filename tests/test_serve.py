@@ -83,3 +83,21 @@ def test_requests_overlap_and_batch():
     assert st["completed"] == 12
     assert st["batches"] < 12  # requests that queued together were measured together
     assert max(bs for _, _, bs in res) > 1
+
+
+@pytest.mark.gpu
+def test_budget_counts_memory_the_batch_pool_keeps():
+    """Batches return their memory to a pool that keeps it for the next
+    batch; a server created afterwards counts that idle memory as free, and
+    a context allocation gets it back from the pool when the device is full."""
+    from wloop_b200._native import lib
+    from wloop_b200.api import Batch
+    items = [((16, 8, 8, 8), 3, P)] * 4
+    with Batch(items, "mixed") as b:
+        b.generate([1, 2, 3, 4], [0.2] * 4)
+        b.run()
+        held = b.device_bytes
+    idle = lib.wlg_batch_pool_idle_bytes(0)
+    assert idle >= held
+    with Server(mem_fraction=0.5) as s:
+        assert s.budget >= 0.5 * idle

@@ -112,6 +112,7 @@ def _load():
         "wlg_batch_set_contract_shape": (i, [vp, i, i, i, i]),
         "wlg_plaq_sum_noalloc": (i, [vp, ip, i, vp, vp]),
         "wlg_batch_use_graph": (i, [vp, i]),
+        "wlg_batch_pool_idle_bytes": (C.c_longlong, [i]),
         "wlg_batch_estimate_bytes": (C.c_longlong, [i, ip, ip, C.POINTER(WlgParms), i]),
         "wlg_server_create": (i, [i, d, i, i, C.POINTER(vp)]),
         "wlg_server_destroy": (i, [vp]),

@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "internal.h"
@@ -79,6 +80,48 @@ struct wlg_batch {
   float last_ms = 0.f;
   int kernels = 0;
 };
+
+namespace {
+
+// Device memory of batches comes from one stream-ordered pool per device
+// that keeps freed memory (release threshold: never): a serving loop creates
+// and destroys a batch per group of requests, and cudaMalloc / cudaFree would
+// cost an allocation round trip and a device-wide synchronisation each time,
+// stalling the batches of other workers in flight.
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pool[kMaxPoolDevices] = {nullptr};
+
+cudaMemPool_t batch_pool(int dev) {
+  if (dev < 0 || dev >= kMaxPoolDevices) return nullptr;
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pool[dev] = p;
+  }
+  return g_pool[dev];
+}
+
+// stream-ordered allocation on the batch's stream; on failure the pool's
+// idle memory is given back to the device and the allocation tried once more
+template <class P>
+int pool_alloc(wlg_batch* b, P** ptr, size_t bytes);
+
+template <class P>
+void pool_free(wlg_batch* b, P*& ptr);
+
+}  // namespace
 
 namespace {
 
@@ -460,14 +503,39 @@ void layout(wlg_batch* b) {
   b->staging_bytes = maxv * 4 * 144;
 }
 
+template <class P>
+int pool_alloc(wlg_batch* b, P** ptr, size_t bytes) {
+  *ptr = nullptr;
+  cudaMemPool_t pool = batch_pool(b->dev);
+  if (!pool) return -1;
+  void* p = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, b->st);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamSynchronize(b->st);
+    cudaMemPoolTrimTo(pool, 0);
+    e = cudaMallocFromPoolAsync(&p, bytes, pool, b->st);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return -1;
+    }
+  }
+  *ptr = static_cast<P*>(p);
+  return 0;
+}
+
+template <class P>
+void pool_free(wlg_batch* b, P*& ptr) {
+  if (ptr) cudaFreeAsync(ptr, b->st);
+  ptr = nullptr;
+}
+
 int ensure_pbuf(wlg_batch* b) {
   if (b->pbuf && b->pbuf_cap >= b->pbuf_bytes) return 0;
-  if (b->pbuf) cudaFree(b->pbuf);
-  b->pbuf = nullptr;
+  pool_free(b, b->pbuf);
   b->pbuf_cap = 0;
-  if (cudaMalloc(&b->pbuf, std::max<size_t>(256, b->pbuf_bytes)) != cudaSuccess) {
+  if (pool_alloc(b, &b->pbuf, std::max<size_t>(256, b->pbuf_bytes))) {
     set_error("batch: cannot allocate %zu bytes of partial sums", b->pbuf_bytes);
-    cudaGetLastError();
     return -1;
   }
   b->pbuf_cap = std::max<size_t>(256, b->pbuf_bytes);
@@ -480,11 +548,14 @@ int build(wlg_batch* b) {
     build_ops<double>(b);
   else
     build_ops<float>(b);
-  if (b->tables) cudaFree(b->tables);
-  b->tables = nullptr;
-  WLG_CUDA(cudaMalloc(&b->tables, std::max<size_t>(256, b->host_tables.size())));
-  WLG_CUDA(cudaMemcpy(b->tables, b->host_tables.data(), b->host_tables.size(),
-                      cudaMemcpyHostToDevice));
+  pool_free(b, b->tables);
+  if (pool_alloc(b, &b->tables, std::max<size_t>(256, b->host_tables.size()))) {
+    set_error("batch: cannot allocate the argument tables");
+    return -1;
+  }
+  WLG_CUDA(cudaMemcpyAsync(b->tables, b->host_tables.data(), b->host_tables.size(),
+                           cudaMemcpyHostToDevice, b->st));
+  WLG_CUDA(cudaStreamSynchronize(b->st));  // host_tables may change after this
   b->built = true;
   return 0;
 }
@@ -509,8 +580,7 @@ int capture(wlg_batch* b) {
 void unbuild(wlg_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
-  if (b->tables) cudaFree(b->tables);
-  b->tables = nullptr;
+  pool_free(b, b->tables);
   b->exec = nullptr;
   b->graph = nullptr;
   b->built = false;
@@ -563,15 +633,17 @@ int wlg_batch_create(int nconf, const int* dims, const int* bcs, const wlg_wloop
     delete b;
     return -1;
   }
-  if (ensure_pbuf(b) || cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&b->arena, b->arena_bytes) != cudaSuccess ||
-      cudaMalloc(&b->staging, b->staging_bytes) != cudaSuccess ||
+  if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess || ensure_pbuf(b) ||
+      pool_alloc(b, &b->arena, b->arena_bytes) || pool_alloc(b, &b->staging, b->staging_bytes) ||
       cudaMallocHost(&b->wl_host, b->wl_host_doubles * sizeof(double)) != cudaSuccess) {
     set_error("batch_create: cannot allocate %.2f GB arena: %s", b->arena_bytes / 1e9,
               cudaGetErrorString(cudaGetLastError()));
     wlg_batch_destroy(b);
     return -1;
   }
+  // the allocations are ordered on the batch's stream; complete them before
+  // the host hands the buffers to copies on other streams
+  WLG_CUDA(cudaStreamSynchronize(b->st));
   cudaEventCreate(&b->ev0);
   cudaEventCreate(&b->ev1);
   *out = b;
@@ -581,18 +653,48 @@ int wlg_batch_create(int nconf, const int* dims, const int* bcs, const wlg_wloop
 int wlg_batch_destroy(wlg_batch* b) {
   if (!b) return 0;
   cudaSetDevice(b->dev);
-  if (b->st) cudaStreamSynchronize(b->st);
-  unbuild(b);
-  if (b->arena) cudaFree(b->arena);
-  if (b->pbuf) cudaFree(b->pbuf);
-  if (b->tables) cudaFree(b->tables);
-  if (b->staging) cudaFree(b->staging);
+  if (b->st) {
+    cudaStreamSynchronize(b->st);
+    unbuild(b);
+    pool_free(b, b->arena);
+    pool_free(b, b->pbuf);
+    pool_free(b, b->staging);
+    cudaStreamSynchronize(b->st);  // the frees are ordered on the stream
+  }
   if (b->wl_host) cudaFreeHost(b->wl_host);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
   return 0;
+}
+
+}  // extern "C"
+
+namespace wlg {
+void batch_pool_trim(int dev) {
+  if (dev < 0 || dev >= kMaxPoolDevices) return;
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    pool = g_pool[dev];
+  }
+  if (pool) cudaMemPoolTrimTo(pool, 0);
+}
+}  // namespace wlg
+
+extern "C" {
+
+long long wlg_batch_pool_idle_bytes(int device) {
+  cudaMemPool_t pool = batch_pool(device);
+  if (!pool) return 0;
+  uint64_t reserved = 0, used = 0;
+  if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return reserved > used ? (long long)(reserved - used) : 0;
 }
 
 int wlg_batch_size(wlg_batch* b) { return b ? (int)b->cfg.size() : 0; }

@@ -88,6 +88,14 @@ static int ensure(DevBuf& b, size_t bytes) {
   if (bytes == 0) return 0;
   cudaError_t e = cudaMalloc(&b.p, bytes);
   if (e != cudaSuccess) {
+    // memory kept idle by the batch pool counts as free: return it, retry
+    cudaGetLastError();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    batch_pool_trim(dev);
+    e = cudaMalloc(&b.p, bytes);
+  }
+  if (e != cudaSuccess) {
     set_error("cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
     cudaGetLastError();
     return -1;

@@ -130,6 +130,10 @@ RArgs reduce_args(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mw
 void contract_reduce_batch(const RArgs* A, const long long* pre, int n, long long total,
                            cudaStream_t st);
 
+// ---- batch memory pool (batch.cu) -------------------------------------------
+// gives the idle memory the batch pool of device dev keeps back to the device
+void batch_pool_trim(int dev);
+
 // ---- layout (layout.cu) ---------------------------------------------------
 // AoS lexicographic FP64 [V][4][18] <-> SoA field of type T (directions [mu0,mu1)).
 template <class T>

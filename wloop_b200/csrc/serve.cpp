@@ -7,8 +7,8 @@
 // FIFO queue.  max_inflight worker threads each repeatedly take the oldest
 // pending request together with further pending requests of the same lattice
 // and precision (up to max_batch), as long as their device footprint fits both
-// the server's memory budget (a fraction of the HBM free at start, minus what
-// the batches in flight reserve) and what cudaMemGetInfo reports free now.
+// the server's memory budget (a fraction of the HBM free at start, counting
+// the batch pool's idle memory, minus what the batches in flight reserve) and what cudaMemGetInfo reports free now.
 // The group becomes one wlg_batch on the worker's own stream: requests that
 // arrive while others run are admitted as soon as a worker and memory free up,
 // and the batches of different workers overlap on the device.  Each request's
@@ -110,10 +110,13 @@ void worker(wlg_server* s) {
         s->cv_done.notify_all();
         continue;
       }
-      size_t fr = 0, tot = 0;
-      cudaMemGetInfo(&fr, &tot);
-      if (s->reserved + head->bytes > s->budget || (long long)fr < head->bytes) {
-        if (s->reserved == 0 && (long long)fr < head->bytes) {
+      size_t fr0 = 0, tot = 0;
+      cudaMemGetInfo(&fr0, &tot);
+      // free for a batch: the device's free memory plus what the batch pool
+      // keeps idle from earlier batches
+      const long long fr = (long long)fr0 + wlg_batch_pool_idle_bytes(s->dev);
+      if (s->reserved + head->bytes > s->budget || fr < head->bytes) {
+        if (s->reserved == 0 && fr < head->bytes) {
           // nothing of ours is in flight: the device is full for other reasons
           s->pending.pop_front();
           fail_locked(s, head, "not enough free device memory");
@@ -127,7 +130,7 @@ void worker(wlg_server* s) {
         Req* q = s->reqs[*it];
         if (group.empty() || (same_shape(group[0]->r, q->r) &&
                               s->reserved + need + q->bytes <= s->budget &&
-                              need + q->bytes <= (long long)fr)) {
+                              need + q->bytes <= fr)) {
           group.push_back(q);
           need += q->bytes;
           it = s->pending.erase(it);
@@ -237,7 +240,9 @@ int wlg_server_create(int device, double mem_fraction, int max_inflight, int max
   if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return -1;
   wlg_server* s = new wlg_server();
   s->dev = device;
-  s->budget = (long long)(mem_fraction * (double)fr);
+  // free for batches: the device's free memory and what the batch pool keeps
+  // idle from earlier batches of this process
+  s->budget = (long long)(mem_fraction * ((double)fr + (double)wlg_batch_pool_idle_bytes(device)));
   s->max_batch = max_batch;
   for (int i = 0; i < max_inflight; i++) s->workers.emplace_back(worker, s);
   *out = s;
