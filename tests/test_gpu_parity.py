@@ -200,6 +200,14 @@ CASES = [
                                  alpha_ape=0.5, proj_iter=4)),
     ((4, 4, 4, 6), 3, WloopParms(msl=8, nss=[1, 1, 0, 1, 1, 1, 0, 1], mwlt=3, mwlr=3,
                                  op_smear=HYP, alpha_hyp=(0.6, 0.3), proj_iter=3)),
+    # the largest loops the parameters allow (mwlt = N0/2+1, mwlr = min Nk/2+1,
+    # wloop_parms.c:174-176): temporal and spatial lines wrap around the
+    # periodic lattice, and with open bc every loop longer than the remaining
+    # time extent vanishes
+    ((8, 4, 6, 4), 3, WloopParms(msl=2, nss=[0, 3], mwlt=5, mwlr=3, op_smear=APE, alpha_ape=0.5,
+                                 proj_iter=4)),
+    ((8, 4, 6, 4), 0, WloopParms(msl=2, nss=[2, 1], mwlt=5, mwlr=3, op_smear=APE, alpha_ape=0.45,
+                                 proj_iter=4)),
 ]
 
 
@@ -216,7 +224,7 @@ def test_wloop_sum_fp64(case):
     assert np.abs(plaq - ref_plaq).max() / np.abs(ref_plaq).max() < 1e-12
 
 
-@pytest.mark.parametrize("case", [0, 1, 3, 4, 6, 8])
+@pytest.mark.parametrize("case", [0, 1, 3, 4, 6, 8, 9, 10])
 def test_wloop_sum_mixed(case):
     n, bc, p = CASES[case]
     u = generate_links(n, bc, 100 + case, 0.25)
