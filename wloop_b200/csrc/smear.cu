@@ -97,7 +97,7 @@ template <class T> __device__ __forceinline__ void hyp_l2_item(const SArgs<T>& A
   int pmn = hyp_pair(mu, nu);
   M3<T> S, u;
   zero(S);
-#pragma unroll
+#pragma unroll 1  // one staple body in the code: the unrolled planes overflow the instruction cache
   for (int rho = 0; rho < 4; rho++) {
     if (rho == mu || rho == nu) continue;
     add_staples(S, g, x, s, fld<T>(A.aux0, g.vol, pmn, rho, 4),
@@ -124,7 +124,7 @@ template <class T> __device__ __forceinline__ void hyp_l1_item(const SArgs<T>& A
   coords(g, s, x);
   M3<T> S, u;
   zero(S);
-#pragma unroll
+#pragma unroll 1
   for (int i = 1; i < 4; i++) {
     int nu = (mu + i) & 3, p = hyp_pair(mu, nu);
     add_staples(S, g, x, s, fld<T>(A.aux1, g.vol, p, nu, 4), fld<T>(A.aux1, g.vol, p, mu, 4), mu,
