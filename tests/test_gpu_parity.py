@@ -181,7 +181,7 @@ def test_hyp_spatial():
 CASES = [
     # (n, bc, parms)
     ((8, 8, 8, 8), 3, WloopParms(msl=4, nss=[0, 5, 5, 5], mwlt=4, mwlr=4, op_smear=APE,
-                                 alpha_ape=0.5, proj_iter=4)),                 # BASELINE c1
+                                 alpha_ape=0.5, proj_iter=4)),                 # the 8^4 workload
     ((8, 4, 6, 4), 0, WloopParms(msl=3, nss=[0, 2, 2], mwlt=5, mwlr=3, op_smear=APE,
                                  alpha_ape=0.5, proj_iter=4)),
     ((6, 4, 4, 4), 3, WloopParms(msl=3, nss=[0, 1, 2], mwlt=4, mwlr=3, op_smear=HYP,

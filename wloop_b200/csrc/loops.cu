@@ -318,8 +318,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // ---- bulk (TMA) copies of whole 32-site tiles into shared memory ----------
 // One-dimensional cp.async.bulk from this GPU's global memory into this
-// CTA's shared memory, completing on an mbarrier (no multicast, no tensor
-// map).  Every wait is bounded: a wait that runs out sets g_stage_timeout,
+// CTA's own shared memory only, completing on an mbarrier (no tensor map).
+// Every wait is bounded: a wait that runs out sets g_stage_timeout,
 // which the host reads after the measurement.
 __device__ int g_stage_timeout;
 
