@@ -8,10 +8,12 @@ benchmark configurations, for the GPU parity tests at full size:
   c1_8x8x8x8_periodic.npz   full wl_mat and |terms| sums (2048 entries)
   c2_24x24x24x48_open.npz   wl_mat and |terms| sums on time slices 0 and 40
                             (4800 entries each) and the per-level plaquettes
+  c3_32x32x32x64_periodic.npz  the same on time slices 0 and 37 (13824
+                            entries each) of the 32^3x64 bench workload
 
 Each file records the sha256 of the generated input field so a test can
-prove it regenerated the same bytes.  Run: python tests/golden/make_golden.py [c1] [c2]
-(c2 takes about ten minutes on 8 cores).
+prove it regenerated the same bytes.  Run: python tests/golden/make_golden.py [c1] [c2] [c3]
+(c2 takes about ten minutes on 8 cores, c3 about two hours).
 """
 import hashlib
 import os
@@ -25,7 +27,7 @@ sys.path.insert(0, ROOT)
 
 from tests import oracle as O  # noqa: E402
 from wloop_b200.api import generate_links  # noqa: E402
-from wloop_b200.workloads import C1, C2  # noqa: E402
+from wloop_b200.workloads import C1, C2, C3  # noqa: E402
 
 
 def field_sha(u):
@@ -59,6 +61,8 @@ def main(which):
         np.savez_compressed(os.path.join(HERE, "c1_8x8x8x8_periodic.npz"), **run(C1))
     if "c2" in which:
         np.savez_compressed(os.path.join(HERE, "c2_24x24x24x48_open.npz"), **run(C2, [0, 40]))
+    if "c3" in which:
+        np.savez_compressed(os.path.join(HERE, "c3_32x32x32x64_periodic.npz"), **run(C3, [0, 37]))
 
 
 if __name__ == "__main__":
