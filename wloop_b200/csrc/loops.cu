@@ -330,6 +330,10 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count)
                : "memory");
 }
+// before the barrier's shared memory goes back to other uses
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_init_fence() {
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
@@ -767,6 +771,10 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
     }
   }
   if (BULK && !stage_ok) mbar_wait_bounded(bar, phase);  // copies still in flight, bounded
+  if (BULK && stage_ok) {  // every phase completed: nothing pending on the barrier
+    __syncwarp();
+    if (lane == 0) mbar_inval(bar);
+  }
   __syncthreads();
   double* out = partial + ((size_t)(x0 * ngrp + grp) * nCB + cb) * rowlen;
   for (int i = threadIdx.x; i < rowlen; i += blockDim.x) {
