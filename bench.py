@@ -194,8 +194,9 @@ def run_ours(args, rank, world, local):
     from wloop_b200.workloads import C3, flops_per_config
 
     from wloop_b200.replicas import Replicas
-    rep = Replicas(backend="nccl" if world > 1 else None)
+    rep = Replicas()
     barrier_max, barrier = rep.max, rep.barrier
+    local = rep.device  # this rank's GPU
 
     w = C3
     if args.lattice:

@@ -224,3 +224,21 @@ def test_run_synthetic_on_gpu(tmp_path):
     with Context(N, 3, "mixed") as ctx:
         ctx.generate(6, 0.2)
         assert np.array_equal(ctx.measure(P), wl[1])
+
+
+def test_merge_refuses_a_short_rank_file(tmp_path):
+    """A rank that failed part-way leaves fewer records than its share; rank 0
+    then refuses to write the merged file (here with a fake two-rank group)."""
+    head = M.dat_head(P, N[0])
+
+    class Rank0:
+        rank, world, local, device = 0, 2, 0, 0
+
+        def barrier(self):
+            pass
+    # rank 1's file: head only, as a rank that died before its first record
+    M.write_head(M.dat_path(str(tmp_path), "s", 1, 2), head)
+    r = M.Run("s", N, 3, P, first=1, last=5)
+    with pytest.raises(WlgError, match="rank 1 wrote 0 of its 2 records"):
+        M.run(r, str(tmp_path), Rank0(), measure=lambda nc: fake_wl(nc, head[0]))
+    assert not os.path.exists(tmp_path / "s.dat")

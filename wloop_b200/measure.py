@@ -218,7 +218,7 @@ def run(r: Run, out_dir: str, replicas: Optional[Replicas] = None,
     <name>.dat after all ranks have finished."""
     rank = replicas.rank if replicas else 0
     world = replicas.world if replicas else 1
-    local = replicas.local if replicas else 0
+    local = replicas.device if replicas else 0
     os.makedirs(out_dir, exist_ok=True)
     head = dat_head(r.parms, r.n[0])
     path = dat_path(out_dir, r.name, rank, world)
@@ -252,6 +252,13 @@ def run(r: Run, out_dir: str, replicas: Optional[Replicas] = None,
         replicas.barrier()
         if rank == 0:
             parts = [dat_path(out_dir, r.name, k, world) for k in range(world)]
+            # a rank that failed leaves fewer records than its share: no merge
+            for k, part in enumerate(parts):
+                want = len(shard(r.configs, k, world))
+                have = count(part)[1]
+                if have != want:
+                    raise WlgError(f"merge: rank {k} wrote {have} of its {want} records "
+                                   f"({part}); the merged file is not written")
             out["merged"] = os.path.join(out_dir, f"{r.name}.dat")
             out["records"] = merge(parts, out["merged"])
         replicas.barrier()

@@ -53,20 +53,27 @@ class Replicas:
         self.rank, self.world, self.local = env_ranks()
         self.dist = None
         self.backend = None
+        self.device = self.local
         if self.world > 1:
             import torch
             import torch.distributed as dist
+            ndev = torch.cuda.device_count() if torch.cuda.is_available() else 0
+            if ndev:
+                # more ranks than visible GPUs share them round-robin; NCCL
+                # cannot hold two ranks of one group on one GPU, so such a
+                # group talks over gloo (its collectives are host decisions only)
+                self.device = self.local % ndev
             if backend is None:
-                backend = "nccl" if torch.cuda.is_available() else "gloo"
+                backend = "nccl" if 0 < ndev and self.world <= ndev else "gloo"
             if backend == "nccl":
-                torch.cuda.set_device(self.local)
+                torch.cuda.set_device(self.device)
             if not dist.is_initialized():
                 dist.init_process_group(backend,
                                         timeout=datetime.timedelta(seconds=timeout_s))
             self.dist, self.backend = dist, backend
 
     def _device(self):
-        return f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        return f"cuda:{self.device}" if self.backend == "nccl" else "cpu"
 
     def barrier(self) -> None:
         if self.dist is not None:
