@@ -57,9 +57,10 @@ def parse():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--lattice", default=None,
                     help="N0xN1xN2xN3 override for small profiling captures (not a bench line)")
-    ap.add_argument("--workload", default="c3", choices=["c3", "c4", "c5"],
-                    help="c3: headline single configuration; c4: 64-configuration batch in one "
-                         "graph launch; c5: serving loop with Poisson arrivals")
+    ap.add_argument("--workload", default="c3", choices=["c3", "c3b", "c4", "c5"],
+                    help="c3: headline single configuration; c3b: 4 configurations of c3 in one "
+                         "graph launch; c4: 64-configuration batch in one graph launch; c5: "
+                         "serving loop with Poisson arrivals")
     ap.add_argument("--requests", type=int, default=100, help="c5: number of requests")
     ap.add_argument("--rate", type=float, default=20.0, help="c5: arrivals per second")
     return ap.parse_args()
@@ -364,7 +365,17 @@ def run_batch(args):
     from wloop_b200.api import Batch, launch_count
     from wloop_b200.autotune import tune_batch
     from wloop_b200.workloads import batch_workloads, flops_per_config
-    ws = batch_workloads()
+    if args.workload == "c3b":
+        import dataclasses
+        from wloop_b200.workloads import C3
+        ws = [dataclasses.replace(C3, seed=C3.seed + i) for i in range(4)]
+        metric = "configs/s, 4 x 32^3x64 (c3) in one graph launch"
+        desc = ("c3 batch: 4 x 32^3x64 periodic, HYP2, APE 0.5 nss 0 10 10 10 10 10, msl 6, "
+                "r<=16, t<=24, one graph launch per step")
+    else:
+        ws = batch_workloads()
+        metric = "configs/s, 64-configuration batch (48 x 16^3x32 + 16 x 24^3x48)"
+        desc = "c4 batch, HYP2 + APE 0.5 nss 0 5 5 5, r,t <= Ns/2, one graph launch per step"
     prec = args.precision
     b = Batch([(w.n, w.bc, w.parms) for w in ws], prec)
     b.generate([w.seed for w in ws], [w.eps for w in ws])
@@ -389,13 +400,12 @@ def run_batch(args):
     ms = e0.elapsed_time(e1) / args.steps
     _, kern = b.stats()
     flops = sum(flops_per_config(w)["total"] for w in ws)
-    line = {"metric": "configs/s, 64-configuration batch (48 x 16^3x32 + 16 x 24^3x48)",
+    line = {"metric": metric,
             "value": len(ws) * 1000.0 / ms, "unit": "configs/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
-            "config": {"workload": "c4 batch, HYP2 + APE 0.5 nss 0 5 5 5, r,t <= Ns/2, one graph "
-                                   "launch per step", "precision": prec,
+            "config": {"workload": desc, "precision": prec,
                        "contract_shape_G_SB_block_nCB": list(shape),
                        "device_bytes": b.device_bytes},
             "kernels_per_graph": kern, "gpu_launches_device_side": kern * args.steps,
@@ -454,7 +464,7 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank)
         return
-    if args.workload == "c4":
+    if args.workload in ("c3b", "c4"):
         run_batch(args)
         return
     if args.workload == "c5":
