@@ -108,3 +108,37 @@ def test_batch_generate_and_shape_change():
         with Context(items[0][0], items[0][1], "mixed") as c:
             c.generate(7, 0.2)
             assert np.array_equal(c.measure(items[0][2]), r0[0])
+
+
+# every batched contraction shape (G bottom levels; SB 1, 2: third form, 0:
+# fourth form, 3: fourth form with unrolled level loops) gives the batch's
+# default result up to summation order, with the line step computed by the
+# form that is launched (a stand-alone stage for the third form, inside the
+# contraction for the fourth)
+BATCH_SHAPES = [(1, 1, 64), (2, 2, 128), (3, 0, 64), (2, 3, 128), (4, 3, 64), (1, 0, 128)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("same_msl", [False, True])
+def test_batch_shapes_agree(prec, same_msl):
+    items = ITEMS if not same_msl else [
+        ((8, 4, 4, 4), 3, WloopParms(msl=4, nss=[0, 1, 1, 2], mwlt=3, mwlr=3, op_smear=APE,
+                                     alpha_ape=0.5, proj_iter=4)),
+        ((6, 4, 6, 4), 0, WloopParms(msl=4, nss=[1, 0, 2, 1], mwlt=3, mwlr=3, op_smear=APE,
+                                     alpha_ape=0.4, proj_iter=3))]
+    fields = [generate_links(n, bc, 500 + i, 0.3) for i, (n, bc, _) in enumerate(items)]
+    with Batch(items, prec) as b:
+        for i, u in enumerate(fields):
+            b.upload(i, u)
+        b.snapshot()
+        b.run()
+        ref = [b.result(i) for i in range(len(items))]
+        for G, SB, block in BATCH_SHAPES:
+            b.set_contract_shape(G=G, SB=SB, nCB=0, block=block)
+            b.restore()
+            b.run()
+            for i in range(len(items)):
+                scale = np.maximum(np.abs(ref[i]), 1e-3)
+                err = np.max(np.abs(b.result(i) - ref[i]) / scale)
+                assert err < (1e-13 if prec == "fp64" else 1e-6), (G, SB, block, i, err)

@@ -1,5 +1,7 @@
 """Golden fixtures (tests/golden/, made by tests/golden/make_golden.py from the
-oracle) at the full sizes of the first two benchmark configurations.
+oracle) at the full sizes of the 8^4, 24^3x48 and 32^3x64 configurations
+(the last is the bench workload: HYP2, 50 APE sweeps over 6 levels, all
+loops r <= 16, t <= 24; two of its 64 time slices are stored).
 
 CPU: the synthetic input is regenerated bit for bit (sha256 of the field),
 and the oracle reproduces the c1 fixture.  GPU: the FP64 path matches every
@@ -14,7 +16,7 @@ import pytest
 
 from tests import oracle as O
 from wloop_b200.api import WloopParms, generate_links
-from wloop_b200.workloads import C1, C2
+from wloop_b200.workloads import C1, C2, C3
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -34,7 +36,10 @@ def field(f):
     return n, int(f["bc"]), generate_links(n, int(f["bc"]), int(f["seed"]), float(f["eps"]))
 
 
-@pytest.mark.parametrize("name", ["c1_8x8x8x8_periodic.npz", "c2_24x24x24x48_open.npz"])
+ALL = ["c1_8x8x8x8_periodic.npz", "c2_24x24x24x48_open.npz", "c3_32x32x32x64_periodic.npz"]
+
+
+@pytest.mark.parametrize("name", ALL)
 def test_fixture_input_regenerates(name):
     f = load(name)
     _, _, u = field(f)
@@ -42,7 +47,7 @@ def test_fixture_input_regenerates(name):
 
 
 def test_fixture_matches_workload_definitions():
-    for name, w in (("c1_8x8x8x8_periodic.npz", C1), ("c2_24x24x24x48_open.npz", C2)):
+    for name, w in zip(ALL, (C1, C2, C3)):
         f = load(name)
         assert tuple(f["n"]) == w.n and int(f["bc"]) == w.bc and int(f["seed"]) == w.seed
         assert int(f["msl"]) == w.parms.msl and list(f["nss"]) == list(w.parms.nss)
@@ -67,7 +72,7 @@ def _check(got, f, tol):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["c1_8x8x8x8_periodic.npz", "c2_24x24x24x48_open.npz"])
+@pytest.mark.parametrize("name", ALL)
 def test_gpu_fp64_matches_fixture(name):
     from wloop_b200 import Context
     f = load(name)
@@ -82,7 +87,7 @@ def test_gpu_fp64_matches_fixture(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["c1_8x8x8x8_periodic.npz", "c2_24x24x24x48_open.npz"])
+@pytest.mark.parametrize("name", ALL)
 def test_gpu_mixed_within_1e6_of_fixture(name):
     from wloop_b200 import Context
     f = load(name)
@@ -95,3 +100,10 @@ def test_gpu_mixed_within_1e6_of_fixture(name):
     err = _check(got, f, 1e-6)
     print(f"{name}: mixed max scaled error {err:.2e}")
     assert err <= 1e-6
+    if name.startswith("c3"):
+        # the headline workload: every stored W within 1e-6 relative of the
+        # FP64 oracle, without the |terms| scale
+        nz = f["wl"] != 0.0
+        rel = np.abs(got - f["wl"])[nz] / np.abs(f["wl"])[nz]
+        print(f"{name}: mixed max relative error {rel.max():.2e}")
+        assert rel.max() <= 1e-6

@@ -461,8 +461,9 @@ int plan(wlg_batch* b) {
   for (Cfg& f : b->cfg) {
     f.cp = contract_plan(f.g, f.p.msl, f.p.mwlt, fp64, b->tG, b->tNCB, b->tBlock);
     // batched forms: SB = 1 or 2 selects the third form, SB = 0 the fourth,
-    // SB = 3 the fourth with its level loops unrolled (msl 4-6)
-    f.cp.SB = b->tG ? b->tSB : 0;
+    // SB = 3 the fourth with its level loops unrolled (msl 4-6; the default in
+    // FP32, as for a single lattice; the unrolled FP64 kernel spills)
+    f.cp.SB = b->tG ? b->tSB : (fp64 ? 0 : 3);
     f.cp.variant = (f.cp.SB == 1 || f.cp.SB == 2) ? 3 : (f.cp.SB == 3 ? 5 : 4);
     if (f.cp.G > 4) {
       set_error("batch: contraction shape G=%d is not available in batched form", f.cp.G);

@@ -1016,7 +1016,10 @@ template <class T>
 void contract_batch(int G, int SB, const CArgs<T>* A, const long long* pre, int n, long long nblocks,
                     int block, size_t smem, int msl, cudaStream_t st) {
   if (n <= 0 || nblocks <= 0) return;
-  if (SB == 0) {  // fourth form (shared-memory reduction)
+  // SB 0: fourth form (shared-memory reduction); SB 3: the same with its level
+  // loops unrolled, where msl (shared by the launch) is 4-6
+  if (SB == 0 || SB == 3) {
+    if (SB == 0) msl = 0;
     switch (G) {
       case 1: launch_contract4_batch<T, 1>(A, pre, n, nblocks, block, smem, msl, st); return;
       case 2: launch_contract4_batch<T, 2>(A, pre, n, nblocks, block, smem, msl, st); return;
