@@ -13,7 +13,7 @@ benchmark configurations, for the GPU parity tests at full size:
 
 Each file records the sha256 of the generated input field so a test can
 prove it regenerated the same bytes.  Run: python tests/golden/make_golden.py [c1] [c2] [c3]
-(c2 takes about ten minutes on 8 cores, c3 about two hours).
+(c2 takes about ten minutes on 8 cores, c3 about 45 minutes).
 """
 import hashlib
 import os
