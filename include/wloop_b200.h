@@ -178,7 +178,9 @@ void* wlg_batch_stream(wlg_batch* b);
 long long wlg_batch_pool_idle_bytes(int device);
 /* contraction shape for the whole batch (0 = automatic); G <= 4; SB selects
  * the form: 1 or 2 the third (SB levels per reduction), 0 the fourth, 3 the
- * fourth with its level loops unrolled (msl 4-6) */
+ * fourth with its level loops unrolled (msl 4-6), 4 the fourth with bulk-copy
+ * staging of the top lines (lattices whose time slice is not a whole number
+ * of 32-site tiles run the fourth) */
 int wlg_batch_set_contract_shape(wlg_batch* b, int G, int SB, int nCB, int block);
 /* on (default): the first run executes directly and captures the pipeline,
  * later runs replay the graph; off: every run executes directly */

@@ -111,11 +111,13 @@ def test_batch_generate_and_shape_change():
 
 
 # every batched contraction shape (G bottom levels; SB 1, 2: third form, 0:
-# fourth form, 3: fourth form with unrolled level loops) gives the batch's
+# fourth form, 3: fourth form with unrolled level loops, 4: fourth form with
+# bulk-copy staging) gives the batch's
 # default result up to summation order, with the line step computed by the
 # form that is launched (a stand-alone stage for the third form, inside the
 # contraction for the fourth)
-BATCH_SHAPES = [(1, 1, 64), (2, 2, 128), (3, 0, 64), (2, 3, 128), (4, 3, 64), (1, 0, 128)]
+BATCH_SHAPES = [(1, 1, 64), (2, 2, 128), (3, 0, 64), (2, 3, 128), (4, 3, 64), (1, 0, 128),
+                (3, 4, 64), (2, 4, 128)]
 
 
 @pytest.mark.gpu

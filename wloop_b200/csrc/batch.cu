@@ -462,9 +462,12 @@ int plan(wlg_batch* b) {
     f.cp = contract_plan(f.g, f.p.msl, f.p.mwlt, fp64, b->tG, b->tNCB, b->tBlock);
     // batched forms: SB = 1 or 2 selects the third form, SB = 0 the fourth,
     // SB = 3 the fourth with its level loops unrolled (msl 4-6; the default in
-    // FP32, as for a single lattice; the unrolled FP64 kernel spills)
-    f.cp.SB = b->tG ? b->tSB : (fp64 ? 0 : 3);
-    f.cp.variant = (f.cp.SB == 1 || f.cp.SB == 2) ? 3 : (f.cp.SB == 3 ? 5 : 4);
+    // FP32, as for a single lattice; the unrolled FP64 kernel spills), SB = 4
+    // the fourth with bulk-copy staging (the FP64 default where a time slice
+    // is whole 32-site tiles; lattices that are not run the fourth form)
+    f.cp.SB = b->tG ? b->tSB : (fp64 ? 4 : 3);
+    if (f.cp.SB == 4 && !contract_can_bulk(f.g)) f.cp.SB = 0;
+    f.cp.variant = (f.cp.SB == 1 || f.cp.SB == 2) ? 3 : (f.cp.SB == 3 ? 5 : (f.cp.SB == 4 ? 7 : 4));
     if (f.cp.G > 4) {
       set_error("batch: contraction shape G=%d is not available in batched form", f.cp.G);
       return -1;
@@ -784,6 +787,12 @@ int wlg_batch_run(wlg_batch* b) {
     set_error("batch_run: %s", cudaGetErrorString(e));
     return -1;
   }
+  bool bulk = false;
+  for (const Cfg& f : b->cfg) bulk = bulk || f.cp.variant == 7;
+  if (bulk && contract_stage_failed() != 0) {
+    set_error("batch_run: the contraction's staged-line copies did not arrive in time");
+    return -1;
+  }
   // the first run executed the kernels directly; later runs replay a graph
   if (b->use_graph && !b->exec && capture(b)) return -1;
   return 0;
@@ -837,7 +846,7 @@ void* wlg_batch_stream(wlg_batch* b) { return b ? (void*)b->st : nullptr; }
 
 int wlg_batch_set_contract_shape(wlg_batch* b, int G, int SB, int nCB, int block) {
   set_error("%s", "");
-  if (!b || G < 0 || G > 4 || SB < 0 || SB > 3 || nCB < 0 ||
+  if (!b || G < 0 || G > 4 || SB < 0 || SB > 4 || nCB < 0 ||
       (block != 0 && (block % 32 != 0 || block > 128))) {
     set_error("batch_set_contract_shape: bad shape");
     return -1;

@@ -789,11 +789,11 @@ __global__ void __launch_bounds__(128, MINB) k_contract4(CArgs<T> A) {
   contract4_body<T, G, MSL, BULK>(A, blockIdx.x);
 }
 
-template <class T, int G, int MSL, int MINB>
+template <class T, int G, int MSL, int MINB, bool BULK>
 __global__ void __launch_bounds__(128, MINB) kb_contract4(const CArgs<T>* __restrict__ A,
                                                           const long long* __restrict__ pre, int n) {
   const int c = find_item(pre, n, (long long)blockIdx.x);
-  contract4_body<T, G, MSL, false>(A[c], (int)(blockIdx.x - pre[c]));
+  contract4_body<T, G, MSL, BULK>(A[c], (int)(blockIdx.x - pre[c]));
 }
 
 // level counts with their own fully unrolled kernels (the usual 4-6); others
@@ -854,11 +854,11 @@ static void launch_contract4(const Geo& g, const ContractPlan& p, const typename
     launch_contract4_b<T, G, false>(g, p, u0, lines, msl, unroll_msl, mwlt, R, partial, level, next, st);
 }
 
-template <class T, int G, int MSL>
+template <class T, int G, int MSL, bool BULK>
 static void launch_contract4_batch_m(const CArgs<T>* A, const long long* pre, int n,
                                      long long nblocks, int block, size_t smem, cudaStream_t st) {
   constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
-  auto kern = kb_contract4<T, G, MSL, MINB>;
+  auto kern = kb_contract4<T, G, MSL, MINB, BULK>;
   static size_t smem_set = 48 * 1024;
   if (smem > smem_set) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -871,12 +871,17 @@ static void launch_contract4_batch_m(const CArgs<T>* A, const long long* pre, in
 // msl: the level count shared by every lattice of the launch, or 0
 template <class T, int G>
 static void launch_contract4_batch(const CArgs<T>* A, const long long* pre, int n, long long nblocks,
-                                   int block, size_t smem, int msl, cudaStream_t st) {
-  switch (msl_variant(msl)) {
-    case 4: launch_contract4_batch_m<T, G, 4>(A, pre, n, nblocks, block, smem, st); break;
-    case 5: launch_contract4_batch_m<T, G, 5>(A, pre, n, nblocks, block, smem, st); break;
-    case 6: launch_contract4_batch_m<T, G, 6>(A, pre, n, nblocks, block, smem, st); break;
-    default: launch_contract4_batch_m<T, G, 0>(A, pre, n, nblocks, block, smem, st); break;
+                                   int block, size_t smem, int msl, bool bulk, cudaStream_t st) {
+  switch (bulk ? 0 : msl_variant(msl)) {
+    case 4: launch_contract4_batch_m<T, G, 4, false>(A, pre, n, nblocks, block, smem, st); break;
+    case 5: launch_contract4_batch_m<T, G, 5, false>(A, pre, n, nblocks, block, smem, st); break;
+    case 6: launch_contract4_batch_m<T, G, 6, false>(A, pre, n, nblocks, block, smem, st); break;
+    default:
+      if (bulk)
+        launch_contract4_batch_m<T, G, 0, true>(A, pre, n, nblocks, block, smem, st);
+      else
+        launch_contract4_batch_m<T, G, 0, false>(A, pre, n, nblocks, block, smem, st);
+      break;
   }
 }
 
@@ -1017,14 +1022,15 @@ void contract_batch(int G, int SB, const CArgs<T>* A, const long long* pre, int 
                     int block, size_t smem, int msl, cudaStream_t st) {
   if (n <= 0 || nblocks <= 0) return;
   // SB 0: fourth form (shared-memory reduction); SB 3: the same with its level
-  // loops unrolled, where msl (shared by the launch) is 4-6
-  if (SB == 0 || SB == 3) {
-    if (SB == 0) msl = 0;
+  // loops unrolled, where msl (shared by the launch) is 4-6; SB 4: the fourth
+  // form with bulk-copy staging (every lattice's time slice whole tiles)
+  if (SB == 0 || SB == 3 || SB == 4) {
+    if (SB != 3) msl = 0;
     switch (G) {
-      case 1: launch_contract4_batch<T, 1>(A, pre, n, nblocks, block, smem, msl, st); return;
-      case 2: launch_contract4_batch<T, 2>(A, pre, n, nblocks, block, smem, msl, st); return;
-      case 3: launch_contract4_batch<T, 3>(A, pre, n, nblocks, block, smem, msl, st); return;
-      case 4: launch_contract4_batch<T, 4>(A, pre, n, nblocks, block, smem, msl, st); return;
+      case 1: launch_contract4_batch<T, 1>(A, pre, n, nblocks, block, smem, msl, SB == 4, st); return;
+      case 2: launch_contract4_batch<T, 2>(A, pre, n, nblocks, block, smem, msl, SB == 4, st); return;
+      case 3: launch_contract4_batch<T, 3>(A, pre, n, nblocks, block, smem, msl, SB == 4, st); return;
+      case 4: launch_contract4_batch<T, 4>(A, pre, n, nblocks, block, smem, msl, SB == 4, st); return;
     }
   }
   if (SB == 2) {
