@@ -360,3 +360,32 @@ def test_prefetched_upload(prec):
         assert np.array_equal(c.measure(p), ref2)
         c.upload_prefetched()
         assert np.array_equal(c.measure(p), ref1)
+
+
+@pytest.mark.parametrize("prec,form", [("fp64", 0), ("fp64", 3), ("mixed", 0), ("mixed", 3)])
+def test_lines_left_by_the_measurement(prec, form):
+    """The spatial lines a measurement leaves (get_pus slots msl..2msl-1) are
+    the products of mwlr level links along each direction, whether the
+    contraction computed them (fourth-form family) or the line-step stage did
+    (third form)."""
+    n, bc, p = CASES[1]
+    u = generate_links(n, bc, 77, 0.25)
+    with Context(n, bc, prec) as c:
+        if form:
+            c.set_contract_tuning(form, 2, 1, 0, 64)
+        c.upload(u)
+        c.measure(p)
+        st = np.array([n[1] * n[2] * n[3], n[2] * n[3], n[3], 1])
+        x = np.indices(n).reshape(4, -1).T
+        for sl in range(p.msl):
+            lev = c.level(sl)
+            got, length = c.lines(sl)
+            assert length == p.mwlr
+            for k in range(3):
+                want = lev[:, k].copy()
+                for step in range(1, length):
+                    y = x.copy()
+                    y[:, k + 1] = (y[:, k + 1] + step) % n[k + 1]
+                    want = want @ lev[y @ st, k]
+                tol = 1e-13 if prec == "fp64" else 2e-6
+                assert np.max(np.abs(got[:, k] - want)) < tol, (sl, k)

@@ -82,6 +82,7 @@ def _load():
         "wlg_wloop_sum": (i, [vp, C.POINTER(WlgParms), dp, dp]),
         "wlg_measure": (i, [vp, C.POINTER(WlgParms), dp, dp]),
         "wlg_download_level": (i, [vp, i, dp]),
+        "wlg_download_lines": (i, [vp, i, dp, ip]),
         "wlg_staple_sum": (i, [ip, dp, dp, i, i, dp]),
         "wlg_project": (i, [dp, i, i]),
         "wlg_set_profiling": (i, [vp, i]),

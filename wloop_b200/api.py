@@ -221,6 +221,15 @@ class Context:
         check(lib.wlg_download_level(self._h, sl, dptr(out.view(np.float64))), "level")
         return out
 
+    def lines(self, sl: int):
+        """Spatial lines of level sl left by the last measurement: (lines of
+        shape (V, 3, 3, 3), their length R = mwlr); get_pus slots msl+sl."""
+        out = np.empty((self.vol, 3, 3, 3), dtype=np.complex128)
+        length = C.c_int(0)
+        check(lib.wlg_download_lines(self._h, sl, dptr(out.view(np.float64)), C.byref(length)),
+              "lines")
+        return out, length.value
+
     # -- timing ---------------------------------------------------------------
     def set_profiling(self, on: bool):
         check(lib.wlg_set_profiling(self._h, int(on)), "set_profiling")
