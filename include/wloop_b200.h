@@ -180,7 +180,8 @@ long long wlg_batch_pool_idle_bytes(int device);
  * the form: 1 or 2 the third (SB levels per reduction), 0 the fourth, 3 the
  * fourth with its level loops unrolled (msl 4-6), 4 the fourth with bulk-copy
  * staging of the top lines (lattices whose time slice is not a whole number
- * of 32-site tiles run the fourth) */
+ * of 32-site tiles run the fourth), 5 SB 3 with the FP32 products as packed
+ * two-lane FMAs (FP32 batches; an FP64 batch runs SB 3) */
 int wlg_batch_set_contract_shape(wlg_batch* b, int G, int SB, int nCB, int block);
 /* on (default): the first run executes directly and captures the pipeline,
  * later runs replay the graph; off: every run executes directly */
@@ -252,8 +253,10 @@ int wlg_reset_kernel_times(wlg_ctx* ctx);
 int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
 /* As above plus the kernel form (2: register-prefetching, 3: staged top
  * lines, shuffle reduction; 4: staged top lines, shared-memory reduction;
- * 5: form 4 with its level loops unrolled for msl 4-6) and SB top levels per
- * reduction (1 or 2; form 3 only). */
+ * 5: form 4 with its level loops unrolled for msl 4-6; 6 / 7: forms 5 / 4
+ * with the top lines staged by bulk copies; 8: form 5 with the FP32
+ * products as packed two-lane FMAs, FP32 contexts only, an FP64 context runs
+ * form 5) and SB top levels per reduction (1 or 2; form 3 only). */
 int wlg_set_contract_tuning(wlg_ctx* ctx, int variant, int G, int SB, int nCB, int block);
 /* The context's CUDA stream (cudaStream_t), for callers that record events. */
 void* wlg_stream(wlg_ctx* ctx);

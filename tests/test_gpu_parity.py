@@ -314,6 +314,8 @@ SHAPES = [  # (form, G, SB, nCB, block)
     # bulk-copy staging (forms 6 and 7; on lattices whose time slices are not
     # whole 32-site tiles they run as forms 5 and 4)
     (6, 3, 0, 0, 128), (6, 2, 0, 5, 32), (7, 3, 0, 0, 64), (7, 1, 0, 0, 96), (6, 4, 0, 3, 64),
+    # packed FP32 products (form 8; an FP64 context runs form 5)
+    (8, 3, 0, 0, 128), (8, 2, 0, 3, 64), (8, 4, 0, 0, 32), (8, 1, 0, 0, 96),
 ]
 
 

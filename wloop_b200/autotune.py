@@ -55,12 +55,13 @@ def candidates(msl: int, fp64: bool, batched: bool) -> List[Shape]:
             continue
         # SB 0: the fourth-form family (shared-memory reduction; its best
         # member for the precision); 1, 2: third form; batches also try SB 3,
-        # the fourth form with its level loops unrolled (FP32, msl 4-6), and
+        # the fourth form with its level loops unrolled (FP32, msl 4-6), SB 5,
+        # the same with packed two-lane FMA products (FP32, msl 4-6), and
         # SB 4, the fourth form with bulk-copy staging (FP64)
         if G == 6:
             sbs = (1,)
         elif batched:
-            sbs = (0, 1, 2) + ((3,) if 4 <= msl <= 6 and not fp64 else ()) + ((4,) if fp64 else ())
+            sbs = (0, 1, 2) + ((3, 5) if 4 <= msl <= 6 and not fp64 else ()) + ((4,) if fp64 else ())
         else:
             sbs = (0, 1, 2)
         for SB in sbs:

@@ -363,7 +363,7 @@ template <class T> void build_ops(wlg_batch* b) {
         gp = &groups.back();
       }
       // unrolled kernels need one level count for the whole launch
-      if (gp->msl != f.p.msl || f.cp.variant != 5) gp->msl = 0;
+      if (gp->msl != f.p.msl || (f.cp.variant != 5 && f.cp.variant != 8)) gp->msl = 0;
       gp->smem = std::max(gp->smem, contract3_smem<T>(f.cp, f.p.msl));
       gp->a.push_back(ca);
       gp->blocks.push_back((long long)f.g.n[0] * f.cp.ngrp * f.cp.nCB);
@@ -461,13 +461,17 @@ int plan(wlg_batch* b) {
   for (Cfg& f : b->cfg) {
     f.cp = contract_plan(f.g, f.p.msl, f.p.mwlt, fp64, b->tG, b->tNCB, b->tBlock);
     // batched forms: SB = 1 or 2 selects the third form, SB = 0 the fourth,
-    // SB = 3 the fourth with its level loops unrolled (msl 4-6; the default in
-    // FP32, as for a single lattice; the unrolled FP64 kernel spills), SB = 4
-    // the fourth with bulk-copy staging (the FP64 default where a time slice
-    // is whole 32-site tiles; lattices that are not run the fourth form)
-    f.cp.SB = b->tG ? b->tSB : (fp64 ? 4 : 3);
+    // SB = 3 the fourth with its level loops unrolled (msl 4-6; the unrolled
+    // FP64 kernel spills), SB = 4 the fourth with bulk-copy staging (the FP64
+    // default where a time slice is whole 32-site tiles; lattices that are not
+    // run the fourth form), SB 5 the unrolled fourth form with packed FP32
+    // products (the eighth form; the FP32 default, as for a single lattice;
+    // an FP64 batch runs SB 3)
+    f.cp.SB = b->tG ? b->tSB : (fp64 ? 4 : 5);
     if (f.cp.SB == 4 && !contract_can_bulk(f.g)) f.cp.SB = 0;
-    f.cp.variant = (f.cp.SB == 1 || f.cp.SB == 2) ? 3 : (f.cp.SB == 3 ? 5 : (f.cp.SB == 4 ? 7 : 4));
+    if (f.cp.SB == 5 && fp64) f.cp.SB = 3;
+    f.cp.variant = (f.cp.SB == 1 || f.cp.SB == 2) ? 3
+                 : (f.cp.SB == 3 ? 5 : (f.cp.SB == 4 ? 7 : (f.cp.SB == 5 ? 8 : 4)));
     if (f.cp.G > 4) {
       set_error("batch: contraction shape G=%d is not available in batched form", f.cp.G);
       return -1;
@@ -846,7 +850,7 @@ void* wlg_batch_stream(wlg_batch* b) { return b ? (void*)b->st : nullptr; }
 
 int wlg_batch_set_contract_shape(wlg_batch* b, int G, int SB, int nCB, int block) {
   set_error("%s", "");
-  if (!b || G < 0 || G > 4 || SB < 0 || SB > 4 || nCB < 0 ||
+  if (!b || G < 0 || G > 4 || SB < 0 || SB > 5 || nCB < 0 ||
       (block != 0 && (block % 32 != 0 || block > 128))) {
     set_error("batch_set_contract_shape: bad shape");
     return -1;

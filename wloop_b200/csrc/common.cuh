@@ -331,6 +331,84 @@ template <class T> __device__ __forceinline__ T retr_dag(const M3<T>& a, const M
   return s + t;
 }
 
+// FP32: the real and the imaginary chain advance together as one packed
+// two-lane FMA (fma.rn.f32x2 of sm_100a, each lane rounded as fmaf); the same
+// products in the same order as the generic form, so the same result.
+template <> __device__ __forceinline__ float retr_dag<float>(const M3<float>& a, const M3<float>& b) {
+  float2 p = __fmul2_rn(a.e[0], b.e[0]);
+#pragma unroll
+  for (int k = 1; k < 9; k++) p = __ffma2_rn(a.e[k], b.e[k], p);
+  return p.x + p.y;
+}
+
+// ---------------------------------------------------------------------------
+// FP32 in-place products of G matrices by one shared matrix, as packed
+// two-lane FMAs: a complex multiply-add c += p q is
+//   {c.re, c.im} += {q.re, q.im} * {p.re, p.re} + {-q.im, q.re} * {p.im, p.im}
+// with the shared factor p in broadcast pairs (formed once per call, used by
+// all G matrices and all three rows or columns) and the per-matrix factor q
+// rotated once per entry.  The products of the scalar forms above, summed in
+// the same k order; within one k the two products of an imaginary part may be
+// added in the other order (FP32 rounding differences only).
+// ---------------------------------------------------------------------------
+// c[g] <- a^dag c[g]   (conj(a_ki) c_kj = {c.re, c.im} a.re + {c.im, -c.re} a.im)
+template <int G>
+__device__ __forceinline__ void lmul_dag_inplace_x2(M3<float> (&c)[G], const M3<float>& a) {
+  float2 ar[9], ai[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    ar[k] = make_float2(a.e[k].x, a.e[k].x);
+    ai[k] = make_float2(a.e[k].y, a.e[k].y);
+  }
+#pragma unroll
+  for (int g = 0; g < G; g++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const float2 x0 = c[g].e[j], x1 = c[g].e[3 + j], x2 = c[g].e[6 + j];
+      const float2 r0 = make_float2(x0.y, -x0.x), r1 = make_float2(x1.y, -x1.x),
+                   r2 = make_float2(x2.y, -x2.x);
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        float2 o = __fmul2_rn(x0, ar[i]);
+        o = __ffma2_rn(r0, ai[i], o);
+        o = __ffma2_rn(x1, ar[3 + i], o);
+        o = __ffma2_rn(r1, ai[3 + i], o);
+        o = __ffma2_rn(x2, ar[6 + i], o);
+        o = __ffma2_rn(r2, ai[6 + i], o);
+        c[g].e[3 * i + j] = o;
+      }
+    }
+}
+
+// c[g] <- c[g] b   (c_ik b_kj = {c.re, c.im} b.re + {-c.im, c.re} b.im)
+template <int G>
+__device__ __forceinline__ void rmul_inplace_x2(M3<float> (&c)[G], const M3<float>& b) {
+  float2 br[9], bi[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    br[k] = make_float2(b.e[k].x, b.e[k].x);
+    bi[k] = make_float2(b.e[k].y, b.e[k].y);
+  }
+#pragma unroll
+  for (int g = 0; g < G; g++)
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const float2 x0 = c[g].e[3 * i], x1 = c[g].e[3 * i + 1], x2 = c[g].e[3 * i + 2];
+      const float2 r0 = make_float2(-x0.y, x0.x), r1 = make_float2(-x1.y, x1.x),
+                   r2 = make_float2(-x2.y, x2.x);
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        float2 o = __fmul2_rn(x0, br[j]);
+        o = __ffma2_rn(r0, bi[j], o);
+        o = __ffma2_rn(x1, br[3 + j], o);
+        o = __ffma2_rn(r1, bi[3 + j], o);
+        o = __ffma2_rn(x2, br[6 + j], o);
+        o = __ffma2_rn(r2, bi[6 + j], o);
+        c[g].e[3 * i + j] = o;
+      }
+    }
+}
+
 template <class D, class S> __device__ __forceinline__ void cvt(M3<D>& d, const M3<S>& s) {
 #pragma unroll
   for (int k = 0; k < 9; k++) {
@@ -353,6 +431,35 @@ __device__ __forceinline__ double det_im(const M3<double>& u) {
   double d3im = (c[3].x * c[7].y + c[3].y * c[7].x) - (c[4].x * c[6].y + c[4].y * c[6].x);
   return (c[0].x * d1im + c[0].y * d1re) - (c[1].x * d2im + c[1].y * d2re) +
          (c[2].x * d3im + c[2].y * d3re);
+}
+
+// c = a*b for a right factor b whose diagonal is real (b.e[0], b.e[4], b.e[8]
+// have zero imaginary parts, as in the projection's X): mul() without the
+// products of those zeros.  Dropping them leaves every sum unchanged (adding
+// a product with an exact zero changes at most the sign of a zero result).
+__device__ __forceinline__ void mul_rdiag(M3<double>& c, const M3<double>& a, const M3<double>& b) {
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      double re, im;
+      if (j == 0) {
+        re = a.e[3 * i].x * b.e[0].x;
+        im = a.e[3 * i].y * b.e[0].x;
+      } else {
+        re = a.e[3 * i].x * b.e[j].x - a.e[3 * i].y * b.e[j].y;
+        im = a.e[3 * i].x * b.e[j].y + a.e[3 * i].y * b.e[j].x;
+      }
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        re = fma(a.e[3 * i + k].x, b.e[3 * k + j].x, re);
+        if (k != j) re = fma(-a.e[3 * i + k].y, b.e[3 * k + j].y, re);
+        if (k != j) im = fma(a.e[3 * i + k].x, b.e[3 * k + j].y, im);
+        im = fma(a.e[3 * i + k].y, b.e[3 * k + j].x, im);
+      }
+      c.e[3 * i + j].x = re;
+      c.e[3 * i + j].y = im;
+    }
 }
 
 #define WLG_SRT18_EPS (4.242640687119285 * 2.220446049250313080847e-16)
@@ -400,7 +507,7 @@ __device__ __forceinline__ void project(M3<double>& u, int iter) {
         x.e[3 * j + i].y = 0.5 * im;
       }
     }
-    mul(y, u, x);
+    mul_rdiag(y, u, x);
     // z = 1 - i Im det(Y) / 3 (projection.c:150-152)
     double zim = det_im(y) * (-1.0 / 3.0);
 #pragma unroll

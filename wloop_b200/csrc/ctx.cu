@@ -420,7 +420,7 @@ template <class T>
 static int do_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, double* plaq) {
   if (do_smear<T>(c, p, plaq) || do_loops<T>(c, p, wl_mat)) return -1;
   WLG_CUDA(cudaStreamSynchronize(c->st));
-  if (c->used_variant >= 6 && contract_stage_failed() != 0) {
+  if ((c->used_variant == 6 || c->used_variant == 7) && contract_stage_failed() != 0) {
     set_error("wloop_sum: the contraction's staged-line copies did not arrive in time");
     return -1;
   }
@@ -887,7 +887,7 @@ int wlg_reset_kernel_times(wlg_ctx* c) {
 
 int wlg_set_contract_tuning(wlg_ctx* c, int variant, int G, int SB, int nCB, int block) {
   CTX_BEGIN(c);
-  if (variant == 1 || variant < 0 || variant > 7 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
+  if (variant == 1 || variant < 0 || variant > 8 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
       nCB < 0 || (block != 0 && (block % 32 != 0 || block > 128)) ||
       (variant == 2 && G == 6 && SB == 2) || (variant >= 3 && G > 4)) {
     set_error("bad contraction tuning (variant %d, G %d, SB %d, nCB %d, block %d)", variant, G,

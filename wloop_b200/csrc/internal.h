@@ -98,7 +98,7 @@ template <class T>
 void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
               const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
               const typename V2<T>::t* level, typename V2<T>::t* next, cudaStream_t st);
-inline bool contract_fuses_lines(const ContractPlan& p) { return p.variant >= 4 && p.variant <= 7; }
+inline bool contract_fuses_lines(const ContractPlan& p) { return p.variant >= 4 && p.variant <= 8; }
 // the bulk-staged forms need time slices of whole 32-site tiles
 inline bool contract_can_bulk(const Geo& g) { return g.vs % 32 == 0; }
 // 1 if a bulk-staged contraction gave up waiting for its copies since the

@@ -238,10 +238,12 @@ ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hin
   p.G = G;
   p.SB = (msl >= 2 && G <= 4 && !(fp64 && G >= 3)) ? 2 : 1;
   // fourth form (staged top lines, shared-memory reduction) unless G = 6,
-  // which only the second form has: in FP32 with its level loops unrolled
-  // (form 5; the unrolled FP64 kernel spills registers), in FP64 with the top
-  // lines staged by bulk copies (form 7; 5 % faster there, 2 % slower in FP32)
-  p.variant = (G <= 4) ? (fp64 ? 7 : 5) : 2;
+  // which only the second form has: in FP32 with its level loops unrolled and
+  // packed two-lane FMA products (form 8; 2-3 % faster than form 5, the same
+  // without the packing, at 32^3x64), in FP64 with the top lines staged by
+  // bulk copies (form 7; 5 % faster there, 2 % slower in FP32; the unrolled
+  // FP64 kernel spills registers)
+  p.variant = (G <= 4) ? (fp64 ? 7 : 8) : 2;
   p.ngrp = (msl + G - 1) / G;
   // FP64 stages twice the bytes per thread: 64-thread blocks keep 3 blocks per SM
   p.block = block_hint > 0 ? block_hint : ((fp64 && p.variant >= 4) ? 64 : 128);
@@ -594,7 +596,9 @@ static void launch_contract3_sb(const Geo& g, const ContractPlan& p, const typen
 // instead of 16-byte cp.async per thread and chunk.  Needs 32-aligned column
 // ranges inside one direction: N1 N2 N3 a multiple of 32 (the launcher
 // checks), column blocks rounded to 32 columns (below).
-template <class T, int G, int MSL, bool BULK>
+// PK (FP32 only): the recursion's products as packed two-lane FMAs
+// (lmul_dag_inplace_x2 / rmul_inplace_x2), the eighth form.
+template <class T, int G, int MSL, bool BULK, bool PK = false>
 __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
   extern __shared__ double acc[];  // [nwarps][mwlt][G][msl] doubles, the line stage, mbarriers
   constexpr int NQ = Chunks<T>::N;
@@ -717,10 +721,15 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
         }
         cp_async_commit();
       }
+      if constexpr (PK && sizeof(T) == 4) {
+        lmul_dag_inplace_x2<G>(C, ua);
+        rmul_inplace_x2<G>(C, ub);
+      } else {
 #pragma unroll
-      for (int gi = 0; gi < G; gi++) lmul_dag_inplace(C[gi], ua);
+        for (int gi = 0; gi < G; gi++) lmul_dag_inplace(C[gi], ua);
 #pragma unroll
-      for (int gi = 0; gi < G; gi++) rmul_inplace(C[gi], ub);
+        for (int gi = 0; gi < G; gi++) rmul_inplace(C[gi], ub);
+      }
       t0 = t1;
       if (tt < mwlt) {
         ld(ua, u0, vol, t0 * vs + xs);
@@ -784,29 +793,29 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
   }
 }
 
-template <class T, int G, int MSL, int MINB, bool BULK>
+template <class T, int G, int MSL, int MINB, bool BULK, bool PK>
 __global__ void __launch_bounds__(128, MINB) k_contract4(CArgs<T> A) {
-  contract4_body<T, G, MSL, BULK>(A, blockIdx.x);
+  contract4_body<T, G, MSL, BULK, PK>(A, blockIdx.x);
 }
 
-template <class T, int G, int MSL, int MINB, bool BULK>
+template <class T, int G, int MSL, int MINB, bool BULK, bool PK>
 __global__ void __launch_bounds__(128, MINB) kb_contract4(const CArgs<T>* __restrict__ A,
                                                           const long long* __restrict__ pre, int n) {
   const int c = find_item(pre, n, (long long)blockIdx.x);
-  contract4_body<T, G, MSL, BULK>(A[c], (int)(blockIdx.x - pre[c]));
+  contract4_body<T, G, MSL, BULK, PK>(A[c], (int)(blockIdx.x - pre[c]));
 }
 
 // level counts with their own fully unrolled kernels (the usual 4-6); others
 // run the generic kernel (MSL = 0)
 static inline int msl_variant(int msl) { return (msl >= 4 && msl <= 6) ? msl : 0; }
 
-template <class T, int G, int MSL, bool BULK>
+template <class T, int G, int MSL, bool BULK, bool PK>
 static void launch_contract4_m(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
                                const typename V2<T>::t* lines, int msl, int mwlt, int R,
                                double* partial, const typename V2<T>::t* level,
                                typename V2<T>::t* next, cudaStream_t st) {
   constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
-  auto kern = k_contract4<T, G, MSL, MINB, BULK>;
+  auto kern = k_contract4<T, G, MSL, MINB, BULK, PK>;
   size_t smem = contract3_smem<T>(p, msl);
   static size_t smem_set = 48 * 1024;
   if (smem > smem_set) {
@@ -830,35 +839,43 @@ static void launch_contract4_m(const Geo& g, const ContractPlan& p, const typena
 }
 
 // unroll_msl: msl to unroll the level loops for, 0 for the generic kernel
-template <class T, int G, bool BULK>
+template <class T, int G, bool BULK, bool PK = false>
 static void launch_contract4_b(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
                                const typename V2<T>::t* lines, int msl, int unroll_msl, int mwlt,
                                int R, double* partial, const typename V2<T>::t* level,
                                typename V2<T>::t* next, cudaStream_t st) {
   switch (msl_variant(unroll_msl)) {
-    case 4: launch_contract4_m<T, G, 4, BULK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
-    case 5: launch_contract4_m<T, G, 5, BULK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
-    case 6: launch_contract4_m<T, G, 6, BULK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
-    default: launch_contract4_m<T, G, 0, BULK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
+    case 4: launch_contract4_m<T, G, 4, BULK, PK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
+    case 5: launch_contract4_m<T, G, 5, BULK, PK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
+    case 6: launch_contract4_m<T, G, 6, BULK, PK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
+    default: launch_contract4_m<T, G, 0, BULK, PK>(g, p, u0, lines, msl, mwlt, R, partial, level, next, st); break;
   }
 }
 
+// pk: packed FP32 products (eighth form; FP32 with cp.async staging only)
 template <class T, int G>
 static void launch_contract4(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
                              const typename V2<T>::t* lines, int msl, int unroll_msl, bool bulk,
-                             int mwlt, int R, double* partial, const typename V2<T>::t* level,
-                             typename V2<T>::t* next, cudaStream_t st) {
+                             bool pk, int mwlt, int R, double* partial,
+                             const typename V2<T>::t* level, typename V2<T>::t* next,
+                             cudaStream_t st) {
+  if constexpr (sizeof(T) == 4) {
+    if (pk) {
+      launch_contract4_b<T, G, false, true>(g, p, u0, lines, msl, unroll_msl, mwlt, R, partial, level, next, st);
+      return;
+    }
+  }
   if (bulk)
     launch_contract4_b<T, G, true>(g, p, u0, lines, msl, unroll_msl, mwlt, R, partial, level, next, st);
   else
     launch_contract4_b<T, G, false>(g, p, u0, lines, msl, unroll_msl, mwlt, R, partial, level, next, st);
 }
 
-template <class T, int G, int MSL, bool BULK>
+template <class T, int G, int MSL, bool BULK, bool PK = false>
 static void launch_contract4_batch_m(const CArgs<T>* A, const long long* pre, int n,
                                      long long nblocks, int block, size_t smem, cudaStream_t st) {
   constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
-  auto kern = kb_contract4<T, G, MSL, MINB, BULK>;
+  auto kern = kb_contract4<T, G, MSL, MINB, BULK, PK>;
   static size_t smem_set = 48 * 1024;
   if (smem > smem_set) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -869,9 +886,21 @@ static void launch_contract4_batch_m(const CArgs<T>* A, const long long* pre, in
 }
 
 // msl: the level count shared by every lattice of the launch, or 0
+// pk: packed FP32 products (eighth form, cp.async staging; FP32 only)
 template <class T, int G>
 static void launch_contract4_batch(const CArgs<T>* A, const long long* pre, int n, long long nblocks,
-                                   int block, size_t smem, int msl, bool bulk, cudaStream_t st) {
+                                   int block, size_t smem, int msl, bool bulk, bool pk,
+                                   cudaStream_t st) {
+  if constexpr (sizeof(T) == 4) {
+    if (pk && !bulk) {
+      switch (msl_variant(msl)) {
+        case 4: launch_contract4_batch_m<T, G, 4, false, true>(A, pre, n, nblocks, block, smem, st); return;
+        case 5: launch_contract4_batch_m<T, G, 5, false, true>(A, pre, n, nblocks, block, smem, st); return;
+        case 6: launch_contract4_batch_m<T, G, 6, false, true>(A, pre, n, nblocks, block, smem, st); return;
+        default: launch_contract4_batch_m<T, G, 0, false, true>(A, pre, n, nblocks, block, smem, st); return;
+      }
+    }
+  }
   switch (bulk ? 0 : msl_variant(msl)) {
     case 4: launch_contract4_batch_m<T, G, 4, false>(A, pre, n, nblocks, block, smem, st); break;
     case 5: launch_contract4_batch_m<T, G, 5, false>(A, pre, n, nblocks, block, smem, st); break;
@@ -893,17 +922,19 @@ void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
     set_error("contract: this form does not compute the next lines");
     return;
   }
-  if (p.variant >= 4 && p.variant <= 7) {
+  if (p.variant >= 4 && p.variant <= 8) {
     // form 5: form 4 with the level loops unrolled for msl 4-6; forms 6 / 7:
     // forms 5 / 4 with the top lines staged by bulk copies, where a time
-    // slice is whole 32-site tiles (else they run as forms 5 / 4)
-    const int m = (p.variant == 5 || p.variant == 6) ? msl : 0;
-    const bool bulk = (p.variant >= 6) && contract_can_bulk(g);
+    // slice is whole 32-site tiles (else they run as forms 5 / 4); form 8:
+    // form 5 with packed FP32 products (the FP64 form runs form 5)
+    const int m = (p.variant == 5 || p.variant == 6 || p.variant == 8) ? msl : 0;
+    const bool bulk = (p.variant == 6 || p.variant == 7) && contract_can_bulk(g);
+    const bool pk = p.variant == 8;
     switch (p.G) {
-      case 1: launch_contract4<T, 1>(g, p, u0, lines, msl, m, bulk, mwlt, R, partial, level, next, st); return;
-      case 2: launch_contract4<T, 2>(g, p, u0, lines, msl, m, bulk, mwlt, R, partial, level, next, st); return;
-      case 3: launch_contract4<T, 3>(g, p, u0, lines, msl, m, bulk, mwlt, R, partial, level, next, st); return;
-      case 4: launch_contract4<T, 4>(g, p, u0, lines, msl, m, bulk, mwlt, R, partial, level, next, st); return;
+      case 1: launch_contract4<T, 1>(g, p, u0, lines, msl, m, bulk, pk, mwlt, R, partial, level, next, st); return;
+      case 2: launch_contract4<T, 2>(g, p, u0, lines, msl, m, bulk, pk, mwlt, R, partial, level, next, st); return;
+      case 3: launch_contract4<T, 3>(g, p, u0, lines, msl, m, bulk, pk, mwlt, R, partial, level, next, st); return;
+      case 4: launch_contract4<T, 4>(g, p, u0, lines, msl, m, bulk, pk, mwlt, R, partial, level, next, st); return;
       default: break;
     }
   }
@@ -1023,14 +1054,16 @@ void contract_batch(int G, int SB, const CArgs<T>* A, const long long* pre, int 
   if (n <= 0 || nblocks <= 0) return;
   // SB 0: fourth form (shared-memory reduction); SB 3: the same with its level
   // loops unrolled, where msl (shared by the launch) is 4-6; SB 4: the fourth
-  // form with bulk-copy staging (every lattice's time slice whole tiles)
-  if (SB == 0 || SB == 3 || SB == 4) {
-    if (SB != 3) msl = 0;
+  // form with bulk-copy staging (every lattice's time slice whole tiles);
+  // SB 5: SB 3 with packed FP32 products (the eighth form; FP64 runs SB 3)
+  if (SB == 0 || SB == 3 || SB == 4 || SB == 5) {
+    if (SB != 3 && SB != 5) msl = 0;
+    const bool bulk = SB == 4, pk = SB == 5;
     switch (G) {
-      case 1: launch_contract4_batch<T, 1>(A, pre, n, nblocks, block, smem, msl, SB == 4, st); return;
-      case 2: launch_contract4_batch<T, 2>(A, pre, n, nblocks, block, smem, msl, SB == 4, st); return;
-      case 3: launch_contract4_batch<T, 3>(A, pre, n, nblocks, block, smem, msl, SB == 4, st); return;
-      case 4: launch_contract4_batch<T, 4>(A, pre, n, nblocks, block, smem, msl, SB == 4, st); return;
+      case 1: launch_contract4_batch<T, 1>(A, pre, n, nblocks, block, smem, msl, bulk, pk, st); return;
+      case 2: launch_contract4_batch<T, 2>(A, pre, n, nblocks, block, smem, msl, bulk, pk, st); return;
+      case 3: launch_contract4_batch<T, 3>(A, pre, n, nblocks, block, smem, msl, bulk, pk, st); return;
+      case 4: launch_contract4_batch<T, 4>(A, pre, n, nblocks, block, smem, msl, bulk, pk, st); return;
     }
   }
   if (SB == 2) {
