@@ -31,18 +31,35 @@ __global__ void k_aos_to_soa(Geo g, const double2* __restrict__ aos, Links<T> U,
   }
 }
 
+// SoA -> AoS through shared memory, one block of 128 threads per 32-site
+// tile: warp q reads direction mu0+q of the tile component by component (one
+// coalesced 512-byte request per component), the block then writes the
+// tile's links in AoS order, consecutive threads on consecutive 16 bytes.
+// Per site the stage holds 4 links (36 double2) plus one double2 of padding,
+// so that eight consecutive lanes writing their sites' entries hit distinct
+// banks.
+constexpr int kSiteStride = 37;  // double2 per site in the stage
 template <class T>
-__global__ void k_soa_to_aos(Geo g, Links<T> U, double2* __restrict__ aos, int mu0, int nmu) {
-  const long long n = (long long)nmu * g.vol;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
-       w += (long long)gridDim.x * blockDim.x) {
-    int q = (int)(w / g.vol), s = (int)(w - (long long)q * g.vol);
-    int mu = mu0 + q;
-    double2* dst = aos + 9 * ((size_t)4 * s + mu);
+__global__ void __launch_bounds__(128) k_soa_to_aos(Geo g, Links<T> U, double2* __restrict__ aos,
+                                                    int mu0, int nmu) {
+  __shared__ double2 tile[32 * kSiteStride];
+  const int s0 = blockIdx.x * 32;
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = s0 + lane;
+  if (q < nmu && s < g.vol) {
     M3<T> m;
-    ld(m, U.p[mu], g.vol, s);
+    ld(m, U.p[mu0 + q], g.vol, s);
+    double2* t = tile + lane * kSiteStride + 9 * q;
 #pragma unroll
-    for (int c = 0; c < 9; c++) dst[c] = make_double2((double)m.e[c].x, (double)m.e[c].y);
+    for (int c = 0; c < 9; c++) t[c] = make_double2((double)m.e[c].x, (double)m.e[c].y);
+  }
+  __syncthreads();
+  const int nsite = min(32, g.vol - s0);
+  const int per = 9 * nmu;  // double2 per site written
+  for (int e = threadIdx.x; e < nsite * per; e += blockDim.x) {
+    const int site = e / per, r = e - site * per;
+    const int mu = r / 9, c = r - mu * 9;
+    aos[9 * ((size_t)4 * (s0 + site) + mu0 + mu) + c] = tile[site * kSiteStride + r];
   }
 }
 
@@ -109,9 +126,9 @@ void aos_to_soa(const Geo& g, const double* aos, Links<T> U, int mu0, int mu1, c
 template <class T>
 void soa_to_aos(const Geo& g, Links<T> U, double* aos, int mu0, int mu1, cudaStream_t st) {
   int nmu = mu1 - mu0;
-  k_soa_to_aos<T><<<grid_n((long long)nmu * g.vol), 256, 0, st>>>(g, U,
-                                                                  reinterpret_cast<double2*>(aos),
-                                                                  mu0, nmu);
+  if (nmu < 1 || nmu > 4) return;
+  k_soa_to_aos<T><<<(g.vol + 31) / 32, 128, 0, st>>>(g, U, reinterpret_cast<double2*>(aos), mu0,
+                                                     nmu);
   WLG_LAUNCH_CHECK("soa_to_aos");
 }
 template <class T>
