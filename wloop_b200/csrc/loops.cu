@@ -750,16 +750,36 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
       } else {
         cp_async_wait_all();
       }
+      if constexpr (PK && sizeof(T) == 4) {
+        // the next level's staged line is read before this level's barrier
+        // (its chunks are overwritten only after its own barrier), so the
+        // shared-memory latency overlaps this level's traces
+        M3<T> ln;
+        ld_stage<T>(ln, myslot, qstride);
 #pragma unroll UNR
-      for (int s2 = 0; s2 < msl; s2++) {
-        M3<T> l;
-        ld_stage<T>(l, myslot + s2 * NQ * qstride, qstride);
-        __syncwarp();  // every lane holds level s2 before its chunks are overwritten
+        for (int s2 = 0; s2 < msl; s2++) {
+          const M3<T> l = ln;
+          if (s2 + 1 < msl) ld_stage<T>(ln, myslot + (s2 + 1) * NQ * qstride, qstride);
+          __syncwarp();  // every lane holds level s2 before its chunks are overwritten
 #pragma unroll
-        for (int gi = 0; gi < G; gi++) {
-          const int row = gi * msl + s2;
-          double* dst = reinterpret_cast<double*>(wchunks + (s2 * NQ + gi) * qstride + (row & 7) * 16);
-          dst[lane] = (double)retr_dag(l, C[gi]);
+          for (int gi = 0; gi < G; gi++) {
+            const int row = gi * msl + s2;
+            double* dst = reinterpret_cast<double*>(wchunks + (s2 * NQ + gi) * qstride + (row & 7) * 16);
+            dst[lane] = (double)retr_dag(l, C[gi]);
+          }
+        }
+      } else {
+#pragma unroll UNR
+        for (int s2 = 0; s2 < msl; s2++) {
+          M3<T> l;
+          ld_stage<T>(l, myslot + s2 * NQ * qstride, qstride);
+          __syncwarp();  // every lane holds level s2 before its chunks are overwritten
+#pragma unroll
+          for (int gi = 0; gi < G; gi++) {
+            const int row = gi * msl + s2;
+            double* dst = reinterpret_cast<double*>(wchunks + (s2 * NQ + gi) * qstride + (row & 7) * 16);
+            dst[lane] = (double)retr_dag(l, C[gi]);
+          }
         }
       }
       __syncwarp();
