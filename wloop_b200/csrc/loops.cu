@@ -238,9 +238,9 @@ ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hin
   p.G = G;
   p.SB = (msl >= 2 && G <= 4 && !(fp64 && G >= 3)) ? 2 : 1;
   // fourth form (staged top lines, shared-memory reduction) unless G = 6,
-  // which only the second form has: in FP32 with its level loops unrolled and
-  // packed two-lane FMA products (form 8; 2-3 % faster than form 5, the same
-  // without the packing, at 32^3x64), in FP64 with the top lines staged by
+  // which only the second form has: in FP32 with its level loops unrolled,
+  // packed two-lane FMA products and the next level's line read ahead (form
+  // 8; 4.6 % faster than form 5 at 32^3x64), in FP64 with the top lines staged by
   // bulk copies (form 7; 5 % faster there, 2 % slower in FP32; the unrolled
   // FP64 kernel spills registers)
   p.variant = (G <= 4) ? (fp64 ? 7 : 8) : 2;
@@ -596,8 +596,9 @@ static void launch_contract3_sb(const Geo& g, const ContractPlan& p, const typen
 // instead of 16-byte cp.async per thread and chunk.  Needs 32-aligned column
 // ranges inside one direction: N1 N2 N3 a multiple of 32 (the launcher
 // checks), column blocks rounded to 32 columns (below).
-// PK (FP32 only): the recursion's products as packed two-lane FMAs
-// (lmul_dag_inplace_x2 / rmul_inplace_x2), the eighth form.
+// PK (FP32 only), the eighth form: the recursion's products as packed
+// two-lane FMAs (lmul_dag_inplace_x2 / rmul_inplace_x2), and each top level's
+// staged line read from shared memory one level ahead.
 template <class T, int G, int MSL, bool BULK, bool PK = false>
 __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
   extern __shared__ double acc[];  // [nwarps][mwlt][G][msl] doubles, the line stage, mbarriers
