@@ -8,6 +8,7 @@
 #include <map>
 #include <string>
 #include <vector>
+#include <nvtx3/nvToolsExt.h>
 #include "internal.h"
 #include "../../include/wloop_b200.h"
 
@@ -143,11 +144,16 @@ static cudaEvent_t get_event(wlg_ctx* c) {
   return e;
 }
 
+// One stage of a measurement: an NVTX range of the stage's name around its
+// launches (profilers select kernels by stage, e.g. ncu --nvtx --nvtx-include
+// "contract/"; without a tool attached the range calls return at once) and,
+// with profiling on, CUDA events on the context's stream around them.
 struct ProfScope {
   wlg_ctx* c;
   const char* name;
   cudaEvent_t a = nullptr;
   ProfScope(wlg_ctx* c_, const char* n) : c(c_), name(n) {
+    nvtxRangePushA(n);
     if (c->prof) {
       a = get_event(c);
       cudaEventRecord(a, c->st);
@@ -159,6 +165,7 @@ struct ProfScope {
       cudaEventRecord(b, c->st);
       c->pending.push_back({name, a, b});
     }
+    nvtxRangePop();
   }
 };
 
