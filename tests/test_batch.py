@@ -39,6 +39,10 @@ def test_autotune_candidates():
     assert all(G <= 4 for G, _, _, _ in candidates(4, False, True))
     assert (6, 1, 64, 0) in candidates(6, False, False)
     assert all(G <= 3 and b == 64 for G, _, b, _ in candidates(6, True, False))
+    # packed-FMA batch shapes (SB 5) for FP32 batches with unrolled level counts only
+    assert any(SB == 5 for _, SB, _, _ in candidates(6, False, True))
+    assert not any(SB == 5 for _, SB, _, _ in candidates(6, True, True))
+    assert not any(SB == 5 for _, SB, _, _ in candidates(3, False, True))
 
 
 @pytest.mark.gpu
