@@ -235,8 +235,13 @@ long long wlg_server_budget(wlg_server* s);
  * Its only scratch is a fixed array inside the library (128 KiB per GPU that
  * loads the library, held until exit), so lattices above
  * WLG_NOALLOC_MAX_SITES sites are rejected.  The first call on a device looks
- * up that array's device address (cudaGetSymbolAddress) and should come
- * before any stream capture.  All calls share the array: calls that overlap
+ * up that array's device address (cudaGetSymbolAddress); with CUDA's lazy
+ * module loading that call also loads the library's module, and the array
+ * with it, onto the device, which needs device memory once.  Make the first
+ * call on each device at start-up, before a preallocated arena claims the
+ * memory and before any stream capture.  links and out must live on the
+ * current device (or be managed memory); a pointer into another GPU's memory
+ * is rejected.  All calls share the array: calls that overlap
  * on the GPU race and must not be issued.  It calls no cudaMalloc, cudaFree
  * or other allocating routine. */
 #define WLG_NOALLOC_MAX_SITES 33554432

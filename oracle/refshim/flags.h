@@ -1,0 +1,6 @@
+/* flags.h -- openQCD-1.4 header name used by the wloop modules; everything is
+ * declared in shim.h (one process, compile-time lattice). */
+#ifndef FLAGS_H
+#define FLAGS_H
+#include "shim.h"
+#endif

@@ -1,0 +1,6 @@
+/* global.h -- openQCD-1.4 header name used by the wloop modules; everything is
+ * declared in shim.h (one process, compile-time lattice). */
+#ifndef GLOBAL_H
+#define GLOBAL_H
+#include "shim.h"
+#endif

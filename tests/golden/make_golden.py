@@ -10,10 +10,16 @@ benchmark configurations, for the GPU parity tests at full size:
                             (4800 entries each) and the per-level plaquettes
   c3_32x32x32x64_periodic.npz  the same on time slices 0 and 37 (13824
                             entries each) of the 32^3x64 bench workload
+  c4_00_16x16x16x32_periodic.npz  configuration 0 of the 64-configuration
+                            batch (16^3x32, its own seed and eps), 8 time
+                            slices of 1296 entries
+  c4_48_24x24x24x48_periodic.npz  configuration 48 of the batch (the first
+                            24^3x48), 8 time slices of 2704 entries
 
 Each file records the sha256 of the generated input field so a test can
 prove it regenerated the same bytes.  Run: python tests/golden/make_golden.py [c1] [c2] [c3]
-(c2 takes about ten minutes on 8 cores, c3 about 45 minutes).
+(c2 takes about ten minutes on 8 cores, c3 about 45 minutes, c4 about
+three minutes).
 """
 import hashlib
 import os
@@ -27,7 +33,7 @@ sys.path.insert(0, ROOT)
 
 from tests import oracle as O  # noqa: E402
 from wloop_b200.api import generate_links  # noqa: E402
-from wloop_b200.workloads import C1, C2, C3  # noqa: E402
+from wloop_b200.workloads import C1, C2, C3, batch_workloads  # noqa: E402
 
 
 def field_sha(u):
@@ -63,6 +69,14 @@ def main(which):
         np.savez_compressed(os.path.join(HERE, "c2_24x24x24x48_open.npz"), **run(C2, [0, 40]))
     if "c3" in which:
         np.savez_compressed(os.path.join(HERE, "c3_32x32x32x64_periodic.npz"), **run(C3, [0, 37]))
+    if "c4" in which:
+        ws = batch_workloads()
+        for i in (0, 48):
+            w = ws[i]
+            n0, ns = w.n[0], w.n[1]
+            slices = sorted({(k * n0) // 8 + (k % 3) for k in range(8)})
+            name = f"c4_{i:02d}_{ns}x{ns}x{ns}x{n0}_periodic.npz"
+            np.savez_compressed(os.path.join(HERE, name), batch_index=i, **run(w, slices))
 
 
 if __name__ == "__main__":

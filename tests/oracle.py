@@ -125,3 +125,25 @@ def wloop_sum(n, bc, u, p, want_abs=False, want_plaq=False, want_levels=False):
     if want_levels:
         out.append(lv)
     return out[0] if len(out) == 1 else tuple(out)
+
+
+def generate_links(n, bc, seed, eps):
+    """The synthetic gauge field from oracle/fieldgen.c, the test-side copy of
+    the product's generator (same bytes; checked in tests/test_reference.py)."""
+    L = lib()
+    if not getattr(L, "_gen_typed", False):
+        L.orc_generate_links.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_uint64, C.c_double,
+                                         C.POINTER(C.c_double)]
+        L.orc_aux_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32]
+        L.orc_aux_uniform.restype = C.c_double
+        L._gen_typed = True
+    vol = int(np.prod(n))
+    u = np.empty((vol, 4, 3, 3), dtype=np.complex128)
+    nn = _n(n)
+    L.orc_generate_links(_i(nn), int(bc), int(seed), float(eps), _d(u.view(np.float64)))
+    return u
+
+
+def aux_uniform(seed, index, tag):
+    generate_links((1, 1, 1, 1), 3, 0, 0.0)  # binds the argument types
+    return lib().orc_aux_uniform(int(seed), int(index), int(tag))

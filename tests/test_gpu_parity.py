@@ -3,8 +3,11 @@
 FP64 bar: every Wilson-loop entry within 1e-12 relative, measured as
 |W_gpu - W_oracle| <= 1e-12 * max(|W_oracle|, A_oracle) with A the oracle's
 sum of |Re tr| over the averaged terms (entries near zero are limited by
-summation order, not by the kernels); entries that are exactly zero in the
-oracle (loops crossing an open boundary) must be exactly zero.  Smeared
+summation order, not by the kernels); the plain relative error is printed
+beside it, with every entry above 1e-12 plain listed with its A/|W| ratio.
+Entries that are exactly zero in the oracle (loops crossing an open
+boundary) must be exactly zero.  Mixed bar: every non-zero entry within 1e-6
+plain relative of the FP64 oracle.  Smeared
 links and plaquettes: 1e-13 absolute per matrix element / 1e-12 relative.
 """
 import numpy as np
@@ -24,7 +27,17 @@ def assert_wl_close(got, ref, ref_abs, tol=TOL_W):
     zero = ref == 0.0
     assert np.all(got[zero] == 0.0), "exact zeros (open-bc crossing loops) must stay exact"
     scale = np.maximum(np.abs(ref), ref_abs)
-    err = np.abs(got - ref)[~zero] / scale[~zero]
+    diff = np.abs(got - ref)[~zero]
+    err = diff / scale[~zero]
+    rel = diff / np.abs(ref)[~zero]
+    print(f"max scaled error {err.max():.2e}, max plain relative error {rel.max():.2e}")
+    # entries above the bar in plain relative terms: each is a near-zero W
+    # whose error is set by summation order, i.e. by sum|terms|/|W|
+    above = np.nonzero(rel > tol)[0]
+    for k in above[:20]:
+        ratio = ref_abs[~zero][k] / abs(ref[~zero][k])
+        print(f"  entry {k}: W {ref[~zero][k]:+.3e}, plain rel {rel[k]:.2e}, "
+              f"sum|terms|/|W| {ratio:.2e}, rel/ratio {rel[k] / ratio:.2e}")
     assert err.max() <= tol, f"max scaled error {err.max():.3e}"
     return err.max()
 
@@ -238,7 +251,9 @@ def test_wloop_sum_mixed(case):
     rel = np.abs(got - ref)[~zero] / np.abs(ref)[~zero]
     scaled = np.abs(got - ref)[~zero] / np.maximum(np.abs(ref), ref_abs)[~zero]
     print(f"mixed vs oracle: max rel {rel.max():.2e}, max scaled {scaled.max():.2e}")
-    assert scaled.max() < 2e-6
+    # the mixed form's bar: every non-zero entry within 1e-6 plain relative
+    # of the FP64 oracle
+    assert rel.max() <= 1e-6, f"max plain relative error {rel.max():.3e}"
 
 
 @pytest.mark.parametrize("bc", [0, 3])

@@ -8,8 +8,13 @@
 // caller passes the gauge field and the result slot in device memory it
 // already owns, and the only scratch the computation needs -- one FP64
 // partial sum per chunk of sites -- lives in the file-scope array below,
-// which the driver allocates once when this module is loaded on a GPU and
-// which every GPU that loads the library holds until the process exits.
+// which the driver allocates when this module is loaded on a GPU and which
+// every GPU that loads the library holds until the process exits.  With
+// CUDA's lazy module loading (the default) the module, and with it the
+// array, is loaded on a device by the first call here on that device (its
+// cudaGetSymbolAddress), so that first call can itself need device memory:
+// make it at start-up, before a preallocated arena claims the memory and
+// before any stream capture.
 //
 // The array is shared by all calls on a device and keeps the last call's
 // contents.  Every partial a call reads is written by that same call first,
@@ -101,8 +106,9 @@ __global__ void __launch_bounds__(kThreads) k_plaq_chunks_total(const double* pa
 }
 
 // device pointer check without touching the memory: a host pointer handed to
-// the kernel would fault or silently read the wrong memory
-int device_accessible(const void* p, const char* what) {
+// the kernel would fault or silently read the wrong memory, and so would
+// device memory of another GPU (no peer access is set up for it)
+int device_accessible(const void* p, const char* what, int dev) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
@@ -111,6 +117,11 @@ int device_accessible(const void* p, const char* what) {
   }
   if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) {
     set_error("wlg_plaq_sum_noalloc: %s must point to device (or managed) memory", what);
+    return 0;
+  }
+  if (a.type == cudaMemoryTypeDevice && a.device != dev) {
+    set_error("wlg_plaq_sum_noalloc: %s lives on device %d, but device %d is current", what,
+              a.device, dev);
     return 0;
   }
   return 1;
@@ -150,7 +161,7 @@ extern "C" int wlg_plaq_sum_noalloc(const double* links, const int n[4], int bc,
     set_error("wlg_plaq_sum_noalloc: no usable current CUDA device");
     return -1;
   }
-  if (!device_accessible(links, "links") || !device_accessible(out, "out")) return -1;
+  if (!device_accessible(links, "links", dev) || !device_accessible(out, "out", dev)) return -1;
   double* partials = nullptr;
   {
     // set-up once per device, with that device current: the device address of
