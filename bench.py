@@ -4,7 +4,8 @@
 One step = one full measurement of one synthetic 32^3x64 configuration, the
 work ms10's set_data does per configuration (main/ms10.c:633-646):
 HYP2 smearing of all links, 6 APE levels (nss 0 10 10 10 10 10, alpha 0.5),
-and the 6x6 Wilson-loop matrices for r <= 16, t <= 24 on every time slice.
+and the 6x6 Wilson-loop matrices for r <= 16, t <= 24 on every time slice,
+plus the plaquette after every smearing level.
 The headline form is mixed precision (FP32 links / staples / line products,
 FP64 projection and sums); the FP64 form runs the same workload and the
 per-entry error of the mixed result against it is reported.
@@ -12,7 +13,8 @@ per-entry error of the mixed result against it is reported.
   value    configs/s with the input field resident in HBM (device-to-device
            restore of the unsmeared field at the start of each step)
   e2e      configs/s through the public API from a pinned host buffer: the
-           FP64 su3_dble field (H2D) in, the wl_mat (D2H) out, every step;
+           FP64 su3_dble field (H2D) in, the wl_mat and plaquettes (D2H)
+           out, every step;
            the next step's field is copied while the current one is
            measured (Context.prefetch / upload_prefetched)
   roofline the Wilson-loop contraction kernel (the dominant kernel), its
@@ -21,9 +23,14 @@ per-entry error of the mixed result against it is reported.
 Multi-GPU (torchrun): independent replicas, one configuration stream per
 GPU, no collective on the data path ("scaling": "weak").
 
---impl reference times the reference algorithm's CPU implementation (the
-FP64 oracle port, since the reference itself cannot be built here) on a
-bounded sample of the same workload on all host cores.
+cpu_baseline: the oracle (the reference algorithm restated, OpenMP) on all
+host threads, on full-size pieces of the workload; c1_measured_pair: the 8^4
+workload measured whole by the GPU and by the reference itself.
+
+--impl reference times the reference's own CPU implementation: its modules
+compiled from source (oracle/_ref, one process: without MPI the reference
+runs on one core), each step one full-size APE sweep, with HYP and the loop
+stage timed at full size in two further processes meanwhile.
 """
 from __future__ import annotations
 
@@ -59,72 +66,195 @@ def parse():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--lattice", default=None,
                     help="N0xN1xN2xN3 override for small profiling captures (not a bench line)")
-    ap.add_argument("--workload", default="c3", choices=["c3", "c3b", "c4", "c5"],
+    ap.add_argument("--workload", default="c3", choices=["c3", "c3b", "c4", "c5", "c5sweep"],
                     help="c3: headline single configuration; c3b: 4 configurations of c3 in one "
                          "graph launch; c4: 64-configuration batch in one graph launch; c5: "
                          "serving loop with Poisson arrivals")
     ap.add_argument("--requests", type=int, default=100, help="c5: number of requests")
     ap.add_argument("--rate", type=float, default=20.0, help="c5: arrivals per second")
+    ap.add_argument("--sweep-rates", default="1,2,3,4,6", help="c5sweep: arrival rates")
+    ap.add_argument("--sweep-requests", type=int, default=120, help="c5sweep: requests per rate")
+    ap.add_argument("--stable-p99-s", type=float, default=10.0,
+                    help="c5sweep: p99 latency bound of a stable rate (seconds)")
     return ap.parse_args()
 
 
 # ---------------------------------------------------------------------------
-# CPU side: bounded, stage-wise sample of the reference algorithm (oracle)
+# CPU side: the reference itself (oracle/_ref) and the oracle, timed on full-
+# size pieces of the workload.  Nothing here loads the product library: the
+# inputs come from the oracle's copy of the field generator.
 # ---------------------------------------------------------------------------
-def cpu_sample(ns: int, nt: int, threads: int):
-    """Times the FP64 oracle (the reference algorithm restated) on an
-    ns^3 x nt lattice with the workload's per-site parameters: HYP once, one
-    APE sweep, and the loop stage for r,t <= 4 with msl 6.  Every stage is
-    linear in the volume, APE in the sweep count, and the reference's
-    loop contraction costs the same per (r,t) pair (wloop.c:545-571), so
-    t_config = (V/V_s) (t_hyp + 50 t_ape + (16*24/16) t_loop)."""
-    from tests import oracle as O  # checker / baseline only
-    from wloop_b200.api import WloopParms, generate_links
-    from wloop_b200.workloads import C3
-    O.set_threads(threads)
-    n = (nt, ns, ns, ns)
-    u = generate_links(n, 3, 3, 0.2)
+class _Parms:
+    """The workload's wloop parameters, without importing the product package
+    (whose import loads libwloop_b200.so)."""
+
+    def __init__(self, msl, nss, mwlt, mwlr):
+        self.msl, self.nss, self.mwlt, self.mwlr = msl, list(nss), mwlt, mwlr
+        self.op_smear, self.alpha_action, self.alpha_ape = 0, (1.0, 1.0, 0.5), 0.5
+        self.alpha_hyp, self.proj_iter, self.proj = (0.0, 0.0), 4, 1
+
+
+C3_N, C3_BC, C3_SEED, C3_EPS = (64, 32, 32, 32), 3, 3, 0.2
+C3_P = _Parms(6, [0, 10, 10, 10, 10, 10], 24, 16)
+C1_N, C1_BC, C1_SEED, C1_EPS = (8, 8, 8, 8), 3, 1, 0.3
+C1_P = _Parms(4, [0, 5, 5, 5], 4, 4)
+C3_DESC = ("c3: 32^3x64 periodic, eps 0.2, HYP2 (1,1,0.5) proj 4, APE 0.5 nss 0 10 10 10 10 10, "
+           "msl 6, r<=16, t<=24")
+
+
+def _loop_piece(p, mwlt):
+    """wloop_sum parameters of one loop piece: all msl levels with no sweeps
+    (the smearing is timed on its own), r = 1, t = 1..mwlt."""
+    return _Parms(p.msl, [0] * p.msl, mwlt, 1)
+
+
+def _piece_worker(mwlt, n, bc, seed, eps, p, q):
+    """Full-size pieces of the reference in their own process: hyp_links once,
+    then the loop stage for r = 1, t = 1..mwlt on the HYP-smeared field.
+    Puts {name: seconds}."""
+    sys.path.insert(0, ROOT)
+    from tests import oracle as O
+    O.set_threads(1)
+    u = O.generate_links(n, bc, seed, eps)
+    from tests import refimpl as R
+    ref = R.Ref(n)
+    ref.set_field(bc, u)
+    out = {}
     t0 = time.perf_counter()
-    uh = O.hyp_links(n, 3, u, 1.0, 1.0, 0.5, 1, 4)
-    t1 = time.perf_counter()
-    O.ape_links(n, uh, 0.5, 1, 4, time=0, nsweeps=1)
-    t2 = time.perf_counter()
-    p = WloopParms(msl=6, nss=[0] * 6, mwlt=4, mwlr=4, alpha_ape=0.5, proj_iter=4)
-    O.wloop_sum(n, 3, uh, p)
-    t3 = time.perf_counter()
-    c3 = C3.parms
-    scale_v = C3.volume / float(nt * ns ** 3)
-    sweeps = sum(c3.nss[:c3.msl])
-    pairs = (c3.mwlr * c3.mwlt) / 16.0
-    t_cfg = scale_v * ((t1 - t0) + sweeps * (t2 - t1) + pairs * (t3 - t2))
-    sample = (f"oracle on {ns}^3x{nt} (1/{scale_v:.1f} of the volume): HYP once "
-              f"{t1 - t0:.2f}s, one APE sweep {t2 - t1:.2f}s, loops r,t<=4 msl 6 {t3 - t2:.2f}s; "
-              f"scaled by volume, {sweeps} sweeps and {pairs:.0f}x the (r,t) pairs")
-    return 1.0 / t_cfg, t3 - t0, sample
+    ref.hyp_links(*p.alpha_action, p.proj, p.proj_iter)
+    out[f"hyp_{mwlt}"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ref.wloop_sum(_loop_piece(p, mwlt))
+    out[f"loops_t{mwlt}"] = time.perf_counter() - t0
+    q.put(out)
+
+
+def _reference_c1(reps):
+    """The 8^4 workload measured whole by the reference: seconds per
+    configuration (ms10's set_data: hyp_links + wloop_sum)."""
+    from tests import oracle as O
+    from tests import refimpl as R
+    ref = R.Ref(C1_N)
+    u = O.generate_links(C1_N, C1_BC, C1_SEED, C1_EPS)
+    ts = []
+    for _ in range(reps):
+        ref.set_field(C1_BC, u)
+        t0 = time.perf_counter()
+        ref.measure(C1_P)
+        ts.append(time.perf_counter() - t0)
+    return statistics.median(ts)
 
 
 def run_reference(args, rank):
+    """The reference's own CPU implementation (oracle/_ref: its modules built
+    from source; one process, as without MPI) on the 32^3x64 workload.  Every
+    piece runs at the full size: each step is one spatial APE sweep of the
+    32^3x64 field (the ms10 run does 50); HYP and the loop stage for
+    (r=1, t=1) and for (r=1, t=1,2) run once each, in two further processes
+    (one core each) while the steps run.  The configs/s is then an estimate from measured pieces:
+    t_config = t_hyp + 50 t_ape + (t_fixed + 384 t_pair), with t_pair =
+    t(t<=2) - t(t<=1) and t_fixed = t(t<=1) - t_pair (the reference's loop
+    stage costs the same for every (r,t) pair at fixed msl, wloop.c:545-571;
+    r <= 16, t <= 24 is 384 pairs)."""
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
-    times, samples = [], ""
+    import multiprocessing as mp
+    from tests import oracle as O
+    from tests import refimpl as R
+    p = C3_P
+    if not R.available(C3_N):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref was not built for 64x32x32x32 (make -C oracle ref)"}))
+        return
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_piece_worker, args=(k, C3_N, C3_BC, C3_SEED, C3_EPS, p, q))
+             for k in (1, 2)]
+    wall0 = time.perf_counter()
+    for pr in procs:
+        pr.start()
+    O.set_threads(os.cpu_count() or 1)
+    u = O.generate_links(C3_N, C3_BC, C3_SEED, C3_EPS)
+    ref = R.Ref(C3_N)
+    ref.set_field(C3_BC, u)
+    steps = []
     for i in range(args.warmup + args.steps):
-        v, wall, samples = cpu_sample(12, 24, threads)
+        t0 = time.perf_counter()
+        ref.ape_links(p.alpha_ape, p.proj, p.proj_iter, time=0, nsweeps=1)
+        dt = time.perf_counter() - t0
         if i >= args.warmup:
-            times.append(1.0 / v)
-    t = statistics.mean(times)
-    value = 1.0 / t
+            steps.append(dt)
+    pieces = {}
+    for _ in procs:
+        pieces.update(q.get())
+    for pr in procs:
+        pr.join()
+    pieces["hyp"] = 0.5 * (pieces["hyp_1"] + pieces["hyp_2"])
+    t_c1 = _reference_c1(3)
+    t_ape = statistics.mean(steps)
+    sweeps = sum(p.nss[:p.msl])
+    pairs = p.mwlr * p.mwlt
+    t_pair = pieces["loops_t2"] - pieces["loops_t1"]
+    t_fixed = pieces["loops_t1"] - t_pair
+    t_cfg = pieces["hyp"] + sweeps * t_ape + t_fixed + pairs * t_pair
+    value = 1.0 / t_cfg
+    sample = (f"the reference's modules built from source (oracle/_ref), one process per piece "
+              f"(one core each), at the full 32^3x64 size: hyp_links {pieces['hyp']:.1f} s "
+              f"(mean of 2); one spatial APE sweep "
+              f"{t_ape:.2f} s (mean of {len(steps)} timed steps; 50 per configuration); loop "
+              f"stage r=1,t=1 {pieces['loops_t1']:.1f} s and r=1,t<=2 {pieces['loops_t2']:.1f} s "
+              f"(per (r,t) pair {t_pair:.1f} s, 384 pairs); configs/s estimated from these "
+              f"measured pieces")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ape * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": "c3: 32^3x64 periodic, HYP2, APE 0.5 nss 0 10 10 10 10 10, "
-                                   "msl 6, r<=16, t<=24", "parallelism": "host threads"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": samples},
+            "config": {"workload": C3_DESC, "parallelism": "one process (the reference "
+                       "without MPI runs on one core)"},
+            "step": "one full-size spatial APE sweep of the reference (ape_spatial_links)",
+            "value_kind": "estimate from full-size measured pieces",
+            "pieces_s": {"hyp": pieces["hyp"], "hyp_runs": [pieces["hyp_1"], pieces["hyp_2"]],
+                         "ape_sweep": t_ape,
+                         "loops_r1_t1": pieces["loops_t1"], "loops_r1_t2": pieces["loops_t2"],
+                         "per_pair": t_pair, "fixed": t_fixed, "config_estimate": t_cfg},
+            "wall_s": time.perf_counter() - wall0,
+            "c1_measured": {"workload": "c1: 8^4 periodic, eps 0.3, HYP2, APE 0.5 nss 0 5 5 5, "
+                                        "msl 4, r,t<=4", "seconds_per_config": t_c1,
+                            "configs_per_s": 1.0 / t_c1, "kind": "reference, whole measurement"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def cpu_sample(threads: int):
+    """The oracle (the reference algorithm restated, OpenMP over sites) on
+    full-size pieces of the 32^3x64 workload on all host threads: hyp once,
+    one spatial APE sweep, the loop stage for (r=1,t=1) and (r=1,t<=2);
+    configs/s estimated as in run_reference."""
+    from tests import oracle as O
+    p = C3_P
+    O.set_threads(threads)
+    u = O.generate_links(C3_N, C3_BC, C3_SEED, C3_EPS)
+    t0 = time.perf_counter()
+    uh = O.hyp_links(C3_N, C3_BC, u, *p.alpha_action, p.proj, p.proj_iter)
+    t1 = time.perf_counter()
+    O.ape_links(C3_N, uh, p.alpha_ape, p.proj, p.proj_iter, time=0, nsweeps=1)
+    t2 = time.perf_counter()
+    O.wloop_sum(C3_N, C3_BC, uh, _loop_piece(p, 1))
+    t3 = time.perf_counter()
+    O.wloop_sum(C3_N, C3_BC, uh, _loop_piece(p, 2))
+    t4 = time.perf_counter()
+    sweeps = sum(p.nss[:p.msl])
+    t_pair = (t4 - t3) - (t3 - t2)
+    t_fixed = (t3 - t2) - t_pair
+    t_cfg = (t1 - t0) + sweeps * (t2 - t1) + t_fixed + p.mwlr * p.mwlt * t_pair
+    sample = (f"oracle on {threads} threads at the full 32^3x64 size: HYP {t1 - t0:.2f} s, one "
+              f"APE sweep {t2 - t1:.3f} s (x{sweeps}), loop stage r=1,t=1 {t3 - t2:.2f} s and "
+              f"r=1,t<=2 {t4 - t3:.2f} s (x{p.mwlr * p.mwlt} pairs); estimated from these "
+              f"measured pieces")
+    return 1.0 / t_cfg, t4 - t0, sample
 
 
 # ---------------------------------------------------------------------------
@@ -217,7 +347,7 @@ def run_ours(args, rank, world, local):
         ctx.snapshot()
         for _ in range(warmup):
             ctx.restore()
-            ctx.measure(p)
+            ctx.measure(p, plaq=True)
         ext = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ctx.reset_kernel_times()
@@ -231,7 +361,7 @@ def run_ours(args, rank, world, local):
         wl = None
         for _ in range(steps):
             ctx.restore()
-            wl = ctx.measure(p)
+            wl, _ = ctx.measure(p, plaq=True)
         e1.record(ext)
         e1.synchronize()
         torch.cuda.synchronize(local)
@@ -258,7 +388,7 @@ def run_ours(args, rank, world, local):
         hnp[...] = ctx.download()
         ctx.prefetch(hnp)
         ctx.upload_prefetched()
-        ctx.measure(p)  # warm the staging buffer
+        ctx.measure(p, plaq=True)  # warm the staging buffer
         ext = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
@@ -273,13 +403,14 @@ def run_ours(args, rank, world, local):
             ctx.upload_prefetched()
             if i + 1 < args.steps:
                 ctx.prefetch(hnp)
-            out = ctx.measure(p)
+            out, pl = ctx.measure(p, plaq=True)
         e1.record(ext)
         e1.synchronize()
         barrier()
         ems = barrier_max(e0.elapsed_time(e1) / args.steps)
         e2e = {"value": world * 1000.0 / ems, "unit": UNIT,
-               "h2d_bytes_per_step": int(hnp.nbytes), "d2h_bytes_per_step": int(out.nbytes),
+               "h2d_bytes_per_step": int(hnp.nbytes),
+               "d2h_bytes_per_step": int(out.nbytes + pl.nbytes),
                "pipelined": "next field's H2D copy overlaps the current measurement"}
     ctx.close()
 
@@ -305,6 +436,16 @@ def run_ours(args, rank, world, local):
     flops_per_launch = (fl["contract"] + fl["lines"]) / p.mwlr
     achieved = flops_per_launch / (per_launch_ms * 1e-3) / 1e12
     peak = peak_tflops(args.precision, local)
+    peak_src = "vector FMA probe measured in this run (wlg_peak_flops, fma.rn.f64; of measured)"
+    peaks_probe = None
+    if args.precision == "mixed":
+        # the kernel issues packed two-lane FMAs: the FP32 roof is the higher
+        # of the scalar and the packed probe
+        p_scalar, p_x2 = peak, peak_tflops("f32x2", local)
+        peaks_probe = {"fma.rn.f32": p_scalar, "fma.rn.f32x2": p_x2}
+        peak = max(p_scalar, p_x2)
+        peak_src = ("vector FMA probe measured in this run (wlg_peak_flops): the higher of "
+                    "scalar fma.rn.f32 and packed fma.rn.f32x2 chains; of measured")
     traffic = load_traffic().get(args.precision)
     peaks_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
     hbm, hbm_src = None, None
@@ -326,10 +467,10 @@ def run_ours(args, rank, world, local):
     roof = {"kernel": "k_contract4 (loop contraction with the fused spatial line step)",
             "bound": "fp32" if args.precision == "mixed" else "fp64",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "peak_source": "vector FMA probe measured in this run (wlg_peak_flops; of measured); "
-                           "the kernel is bound by CUDA-core FMA throughput, not by HBM or "
-                           "tensor cores (3x3 complex products have no tensor-core form), "
-                           "and MEASURED_PEAKS.json has no CUDA-core peak",
+            "peak_source": peak_src + "; the kernel is bound by CUDA-core FMA throughput, not "
+                           "by HBM or tensor cores (3x3 complex products have no tensor-core "
+                           "form), and MEASURED_PEAKS.json has no CUDA-core peak",
+            "peak_probes_tflops": peaks_probe,
             "flops_per_launch": flops_per_launch, "ms_per_launch": per_launch_ms,
             "traffic": traffic,
             "hbm": {"achieved": hbm_ach, "peak": hbm, "unit": "GB/s",
@@ -341,11 +482,25 @@ def run_ours(args, rank, world, local):
     total_ms = sum(v[0] for v in kt.values())
     shares = {k: round(v[0] / total_ms, 4) for k, v in kt.items() if total_ms > 0}
 
+    # ---- mixed result against the FP64 oracle's fixture (two time slices) ----
+    vs_oracle = None
+    fx = os.path.join(ROOT, "tests", "golden", "c3_32x32x32x64_periodic.npz")
+    if not args.lattice and args.precision == "mixed" and os.path.exists(fx):
+        f = np.load(fx)
+        got = wl_main.reshape(w.n[0], -1)[f["x0"]]
+        nz = f["wl"] != 0.0
+        rel = np.abs(got - f["wl"])[nz] / np.abs(f["wl"])[nz]
+        vs_oracle = {"max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
+                     "entries": int(rel.size), "time_slices": [int(x) for x in f["x0"]]}
+
     cpu = None
+    c1 = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         threads = os.cpu_count() or 1
-        v, wall, sample = cpu_sample(16, 32, threads)
+        v, wall, sample = cpu_sample(threads)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        c1 = c1_pair(local)
+
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -359,9 +514,39 @@ def run_ours(args, rank, world, local):
                            "l2": "inputs larger than L2 (field 151-302 MB, level store 1.9-3.8 GB)"},
                 "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
                 "gpu_launches": launches, "fp64_form": fp64, "kernel_share": shares,
+                "mixed_vs_oracle_fixture": vs_oracle, "c1_measured_pair": c1,
                 "algorithmic_flops_per_config": fl["total"]}
         print(json.dumps(line), flush=True)
     rep.close()
+
+
+def c1_pair(device):
+    """The 8^4 workload measured whole on both sides: the GPU through the
+    public API (host field in, wl_mat and plaquettes out, per configuration)
+    in both forms, and the reference itself (oracle/_ref) on one core."""
+    import numpy as np
+    from wloop_b200.api import Context, generate_links
+    from wloop_b200.workloads import C1
+    out = {"workload": "c1: 8^4 periodic, eps 0.3, HYP2, APE 0.5 nss 0 5 5 5, msl 4, r,t<=4"}
+    u = generate_links(C1.n, C1.bc, C1.seed, C1.eps)
+    for prec in ("mixed", "fp64"):
+        with Context(C1.n, C1.bc, prec, device=device) as c:
+            for _ in range(3):
+                c.upload(u)
+                c.measure(C1.parms, plaq=True)
+            reps = 50
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                c.upload(u)
+                c.measure(C1.parms, plaq=True)
+            out[f"gpu_{prec}_configs_per_s"] = reps / (time.perf_counter() - t0)
+    from tests import refimpl as R
+    if R.available(C1.n):
+        t = _reference_c1(3)
+        out["reference_configs_per_s"] = 1.0 / t
+        out["reference_cores"] = 1
+        out["gpu_mixed_over_reference"] = out["gpu_mixed_configs_per_s"] * t
+    return out
 
 
 def run_batch(args):
@@ -422,43 +607,68 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def _serve_once(prec, nreq, rate, seed=5000):
+    """One serving run: nreq c5 requests (volumes from {16^3x32, 24^3x48,
+    32^3x64, 48^3x96}, eps ~ U[0.15,0.35], bc 50/50 open/periodic, HYP2 + 4 APE
+    levels, r,t <= Ns/2) with Poisson arrivals at `rate` per second."""
+    from wloop_b200.api import Server, aux_uniform
+    from wloop_b200.workloads import serving_request
+    reqs = [serving_request(i, seed) for i in range(nreq)]
+    t = 0.0
+    arrivals = []
+    for i in range(nreq):  # exponential inter-arrival times from the seeded stream
+        u = aux_uniform(seed, i, 7)
+        t += -math.log(1.0 - u) / rate
+        arrivals.append(t)
+    with Server(max_inflight=3, max_batch=8, mem_fraction=0.85) as s:
+        t0 = time.perf_counter()
+        ids = []
+        for w, ta in zip(reqs, arrivals):
+            dt = ta - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            ids.append(s.submit(w.n, w.bc, w.parms, prec, seed=w.seed, eps=w.eps))
+        for i in ids:
+            s.wait(i)
+        wall = time.perf_counter() - t0
+        st = s.stats()
+    mix = {}
+    for w in reqs:
+        key = "x".join(str(v) for v in (w.n[1], w.n[1], w.n[1], w.n[0]))
+        mix[key] = mix.get(key, 0) + 1
+    return {"requests": nreq, "rate_per_s": rate, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "configs_per_s": st["throughput"], "batches": st["batches"], "failed": st["failed"],
+            "arrival_span_s": arrivals[-1], "wall_s": wall, "volume_mix": mix}
+
+
 def run_serve(args):
     """c5: measurement requests with Poisson arrivals (rate --rate) over the
     volumes {16^3x32, 24^3x48, 32^3x64, 48^3x96}, eps ~ U[0.15,0.35], bc
     open/periodic 50/50, HYP2 + 4 APE levels, r,t <= Ns/2; p50/p99 latency and
-    throughput for the mixed and the FP64 forms."""
-    import random
-    from wloop_b200.api import Server, aux_uniform
-    from wloop_b200.workloads import serving_request
+    throughput for the mixed and the FP64 forms (the same --requests each).
+    --workload c5sweep adds, per form, runs at increasing arrival rates
+    (--sweep-rates, --sweep-requests each): the saturating throughput is the
+    completion rate at the highest rate, and the highest stable rate is the
+    highest swept rate whose completion rate keeps up with the arrivals (at
+    least 95 %) with p99 below --stable-p99-s."""
     out = {"metric": "serving: p50/p99 latency (ms) and configs/s, Poisson arrivals",
            "unit": "configs/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
            "requests": args.requests, "rate_per_s": args.rate, "forms": {}}
-    for prec, nreq in (("mixed", args.requests), ("fp64", max(10, args.requests // 3))):
-        reqs = [serving_request(i) for i in range(nreq)]
-        t = 0.0
-        arrivals = []
-        for i in range(nreq):  # exponential inter-arrival times from the seeded stream
-            u = aux_uniform(5000, i, 7)
-            t += -math.log(1.0 - u) / args.rate
-            arrivals.append(t)
-        with Server(max_inflight=3, max_batch=8, mem_fraction=0.85) as s:
-            t0 = time.perf_counter()
-            ids = []
-            for w, ta in zip(reqs, arrivals):
-                dt = ta - (time.perf_counter() - t0)
-                if dt > 0:
-                    time.sleep(dt)
-                ids.append(s.submit(w.n, w.bc, w.parms, prec, seed=w.seed, eps=w.eps))
-            for i in ids:
-                s.wait(i)
-            st = s.stats()
-        mix = {}
-        for w in reqs:
-            key = "x".join(str(v) for v in (w.n[1], w.n[1], w.n[1], w.n[0]))
-            mix[key] = mix.get(key, 0) + 1
-        out["forms"][prec] = {"requests": nreq, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-                              "configs_per_s": st["throughput"], "batches": st["batches"],
-                              "failed": st["failed"], "volume_mix": mix}
+    for prec in ("mixed", "fp64"):
+        out["forms"][prec] = _serve_once(prec, args.requests, args.rate)
+    if args.workload == "c5sweep":
+        rates = [float(x) for x in args.sweep_rates.split(",")]
+        out["sweep"] = {}
+        for prec in ("mixed", "fp64"):
+            runs = [_serve_once(prec, args.sweep_requests, r) for r in rates]
+            stable = [r["rate_per_s"] for r in runs
+                      if r["configs_per_s"] >= 0.95 * r["requests"] / r["arrival_span_s"]
+                      and r["p99_ms"] <= 1e3 * args.stable_p99_s]
+            out["sweep"][prec] = {"runs": runs,
+                                  "saturating_configs_per_s": max(r["configs_per_s"] for r in runs),
+                                  "highest_stable_rate_per_s": max(stable) if stable else None,
+                                  "stable_rule": f"completions >= 95% of arrivals per second and "
+                                                 f"p99 <= {args.stable_p99_s} s"}
     out["value"] = out["forms"]["mixed"]["configs_per_s"]
     print(json.dumps(out), flush=True)
 
@@ -474,7 +684,7 @@ def main():
     if args.workload in ("c3b", "c4"):
         run_batch(args)
         return
-    if args.workload == "c5":
+    if args.workload in ("c5", "c5sweep"):
         run_serve(args)
         return
     run_ours(args, rank, world, local)

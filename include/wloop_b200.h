@@ -192,12 +192,15 @@ long long wlg_batch_estimate_bytes(int nconf, const int* dims, const int* bcs,
 
 /* ---- serving: a request loop with continuous batching -----------------------
  * No counterpart in the reference.  Requests queue FIFO; max_inflight worker
- * threads each take the oldest request plus pending requests of the same
- * lattice and precision (up to max_batch) whose device footprint fits the
+ * threads each take the oldest request whose device footprint fits the
  * budget (mem_fraction of the HBM free at creation, minus batches in flight)
- * and the memory free now, and measure them as one wlg_batch on their own
- * stream, so batches of different workers overlap on the device and new
- * requests are admitted as soon as a worker and memory free up. */
+ * and the memory free now, plus later pending requests of the same precision
+ * (any lattices; up to max_batch) that fit as well, and measure them as one
+ * wlg_batch on their own stream, so batches of different workers overlap on
+ * the device and new requests are admitted as soon as a worker and memory
+ * free up.  A head of the queue that does not fit yet is bypassed by later
+ * requests only until it has waited the bypass limit (wlg_server_set_limits),
+ * so it cannot starve. */
 typedef struct {
   int n[4];
   int bc;
@@ -223,6 +226,11 @@ const char* wlg_server_error(void);
 int wlg_server_stats(wlg_server* s, long long* completed, long long* failed, long long* batches,
                      double* p50_ms, double* p99_ms, double* throughput);
 long long wlg_server_budget(wlg_server* s);
+/* Replaces the memory budget (budget_bytes > 0) and the bypass limit
+ * (bypass_ms >= 0; default 5000): a request at the head of the queue that
+ * does not fit yet lets later requests that fit start before it until it has
+ * waited bypass_ms, after which nothing else starts before it. */
+int wlg_server_set_limits(wlg_server* s, long long budget_bytes, double bypass_ms);
 
 /* ---- plaquette sum without device allocation -------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
@@ -286,7 +294,10 @@ int wlg_shift_links(wlg_ctx* ctx, const int s[4]);
  * ends by itself and reports instead of hanging. */
 int wlg_selftest_wait(int device, double limit_s, int* timed_out, double* elapsed_s);
 /* Achievable vector FMA throughput of the device in TFLOP/s (2 flops per
- * FMA), FP64 or FP32 (precision WLG_FP64 / WLG_MIXED). */
+ * FMA), FP64 or FP32 (precision WLG_FP64 / WLG_MIXED), or FP32 through the
+ * packed two-lane FMA fma.rn.f32x2 (WLG_PEAK_F32X2, 2 FMAs per lane and
+ * instruction). */
+#define WLG_PEAK_F32X2 2
 int wlg_peak_flops(int precision, int device, double* tflops);
 
 /* ---- measurement output files (host only) -----------------------------------
@@ -308,6 +319,14 @@ int wlg_dat_read(const char* path, long long rec, int* nc, double* wl_mat, int w
  * compared with the record at byte offset `offset`. */
 int wlg_par_write_wloop(const char* path, const wlg_wloop_parms* p);
 int wlg_par_check_wloop(const char* path, long long offset, const wlg_wloop_parms* p);
+/* boundary-condition part of the .par file, which ms10 writes before the
+ * wloop part (main/ms10.c:290-295, openQCD-1.4's write_bc_parms /
+ * check_bc_parms): int32 bc type, then 10 doubles {cG, cG', cF, cF',
+ * phi[3], phi'[3]} = {1, 1, 1, 1, 0, ...} for bc 0 (open) and 3 (periodic).
+ * The record is restated from openQCD's published format (openQCD is not
+ * vendored with the reference), 84 bytes. */
+int wlg_par_write_bc(const char* path, int bc);
+int wlg_par_check_bc(const char* path, long long offset, int bc);
 
 /* ---- gauge configurations in openQCD's exported format (host only) ---------
  * What ms10 reads with import_cnfg (main/ms10.c:709-718; the format belongs
@@ -315,12 +334,26 @@ int wlg_par_check_wloop(const char* path, long long offset, const wlg_wloop_parm
  * double (the writer's average plaquette), then for every odd point in
  * lexicographic order the 8 links U(x,0), U(x-0,0), ..., U(x,3), U(x-3,3) as
  * su3_dble, little-endian.  links: [V][4][18] doubles, lexicographic sites.
- * The plaquette is passed through as stored, not recomputed or checked.
- * Errors return -1 with the message in wlg_cnfg_error(). */
+ * These file-level calls pass the plaquette through as stored; the context
+ * calls below recompute it.  Errors return -1 with the message in
+ * wlg_cnfg_error(). */
 const char* wlg_cnfg_error(void);
 int wlg_cnfg_read_head(const char* path, int n[4], double* plaq);
 int wlg_cnfg_import(const char* path, const int n[4], double* links, double* plaq);
 int wlg_cnfg_export(const char* path, const int n[4], const double* links, double plaq);
+/* import_cnfg into a context (main/ms10.c:709-718): reads the file (its
+ * extents must be the context's), zeroes the time links of the last slice
+ * with open bc (set_bc), uploads the field and recomputes the average
+ * plaquette on the device in FP64 from the uploaded su3_dble links: the sum
+ * of Re tr U(p) over 6 V plaquettes, or (6 N0 - 3) N1 N2 N3 with open bc.  It
+ * must agree with the value in the file's head within sqrt(nplaq)
+ * DBL_EPSILON, the check openQCD's import_cnfg makes; otherwise -1 with
+ * "Incorrect average plaquette" (wlg_last_error).  plaq (may be NULL) gets
+ * the recomputed value.  wlg_export_cnfg writes the context's field with its
+ * recomputed average plaquette in the head (mixed contexts: the FP32 links
+ * widened to FP64). */
+int wlg_import_cnfg(wlg_ctx* ctx, const char* path, double* plaq);
+int wlg_export_cnfg(wlg_ctx* ctx, const char* path, double* plaq);
 
 #ifdef __cplusplus
 }

@@ -87,6 +87,25 @@ def test_par_layout(tmp_path):
         M.check_par(path, q)
 
 
+def test_par_bc_record_precedes_wloop_record(tmp_path):
+    """The .par file as ms10 writes it (ms10.c:290-313): the boundary-condition
+    record (int32 type, 10 doubles cG, cG', cF, cF', phi[3], phi'[3]) and then
+    the wloop record."""
+    for bc in (0, 3):
+        path = str(tmp_path / f"bc{bc}.par")
+        M.write_par(path, P, bc)
+        raw = open(path, "rb").read()
+        assert len(raw) == M.BC_RECORD_BYTES + 4 * (P.msl + 4) + 8 * 6
+        assert struct.unpack("<i", raw[:4]) == (bc,)
+        assert struct.unpack("<10d", raw[4:84]) == (1.0, 1.0, 1.0, 1.0) + (0.0,) * 6
+        assert struct.unpack(f"<{P.msl}i", raw[84:84 + 4 * P.msl]) == tuple(P.nss[:P.msl])
+        M.check_par(path, P, bc=bc)
+        with pytest.raises(WlgError, match="do not match"):
+            M.check_par(path, P, bc=3 - bc)
+    with pytest.raises(WlgError, match="open"):
+        M.write_par(str(tmp_path / "x.par"), P, 1)
+
+
 def test_shard_covers_every_config_once():
     cfgs = config_numbers(3, 40, 4)
     assert cfgs[0] == 3 and cfgs[-1] <= 40 and len(cfgs) == 10
@@ -103,10 +122,10 @@ def test_run_single_process_with_fake_measure(tmp_path):
     r = M.Run("one", N, 3, P, first=2, last=10, step=2)
     res = M.run(r, str(tmp_path), measure=lambda nc: fake_wl(nc, head[0]))
     assert res["configs"] == [2, 4, 6, 8, 10]
-    h, ncs, wl = M.read(str(tmp_path / "one.dat"))
+    h, ncs, wl = M.read(str(tmp_path / "one.ms10.dat"))
     assert list(ncs) == [2, 4, 6, 8, 10]
     assert np.array_equal(wl[3], fake_wl(8, head[0]))
-    M.check_par(str(tmp_path / "one.par"), P)
+    M.check_par(str(tmp_path / "one.ms10.par"), P, bc=3)
 
 
 # ---------------------------------------------------------------------------
@@ -182,8 +201,8 @@ def test_two_replicas_gloo_merge_equals_single_process(tmp_path):
     single = M.run(M.Run("rep", N, 3, P, first=1, last=9), str(tmp_path / "one"),
                    measure=lambda nc: fake_wl(nc, head[0]))
     assert single["configs"] == list(range(1, 10))
-    a = open(tmp_path / "rep" / "rep.dat", "rb").read()
-    b = open(tmp_path / "one" / "rep.dat", "rb").read()
+    a = open(tmp_path / "rep" / "rep.ms10.dat", "rb").read()
+    b = open(tmp_path / "one" / "rep.ms10.dat", "rb").read()
     assert a == b
 
 
@@ -203,7 +222,7 @@ def test_run_on_gpu_matches_context_and_oracle(tmp_path):
     r = M.Run("g", N, 0, P, first=1, last=3, precision="fp64", eps=0.25)
     fields = {nc: generate_links(N, 0, 100 + nc, 0.25) for nc in r.configs}
     M.run(r, str(tmp_path), source=lambda nc: fields[nc])
-    h, ncs, wl = M.read(str(tmp_path / "g.dat"))
+    h, ncs, wl = M.read(str(tmp_path / "g.ms10.dat"))
     assert list(ncs) == [1, 2, 3]
     with Context(N, 0, "fp64") as ctx:
         for k, nc in enumerate(ncs):
@@ -220,7 +239,7 @@ def test_run_synthetic_on_gpu(tmp_path):
     from wloop_b200 import Context
     r = M.Run("s", N, 3, P, first=5, last=6, precision="mixed", eps=0.2)
     M.run(r, str(tmp_path))
-    h, ncs, wl = M.read(str(tmp_path / "s.dat"))
+    h, ncs, wl = M.read(str(tmp_path / "s.ms10.dat"))
     with Context(N, 3, "mixed") as ctx:
         ctx.generate(6, 0.2)
         assert np.array_equal(ctx.measure(P), wl[1])
@@ -241,4 +260,4 @@ def test_merge_refuses_a_short_rank_file(tmp_path):
     r = M.Run("s", N, 3, P, first=1, last=5)
     with pytest.raises(WlgError, match="rank 1 wrote 0 of its 2 records"):
         M.run(r, str(tmp_path), Rank0(), measure=lambda nc: fake_wl(nc, head[0]))
-    assert not os.path.exists(tmp_path / "s.dat")
+    assert not os.path.exists(tmp_path / "s.ms10.dat")

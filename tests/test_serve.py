@@ -101,3 +101,49 @@ def test_budget_counts_memory_the_batch_pool_keeps():
     assert idle >= held
     with Server(mem_fraction=0.5) as s:
         assert s.budget >= 0.5 * idle
+
+
+def _bypass_run(bypass_ms):
+    """A large request A runs; a second large request B waits at the head of
+    the queue (the budget holds one large and two small requests); small
+    requests C, D behind B.  Returns the completion times of A and C."""
+    big, small = (32, 16, 16, 16), (8, 4, 4, 4)
+    with Server(max_inflight=3, max_batch=1) as s:
+        s.set_limits(budget_bytes=estimate_bytes(big, 3, P, "fp64") +
+                     2 * estimate_bytes(small, 3, P, "fp64") + 1024, bypass_ms=bypass_ms)
+        done = {}
+        t0 = time.perf_counter()
+        ids = {k: (s.submit(n, 3, P, "fp64", seed=k + 1, eps=0.25), time.perf_counter())
+               for k, n in enumerate([big, big, small, small])}
+        for k, (rid, ts) in ids.items():
+            _, lat, _ = s.wait(rid)
+            done[k] = ts - t0 + lat * 1e-3
+        assert s.stats()["failed"] == 0
+    return done[0], done[2]
+
+
+@pytest.mark.gpu
+def test_head_of_line_request_is_bypassed_then_protected():
+    """A small request that fits starts before an older large one that does
+    not fit yet; with a zero bypass limit it waits behind it instead."""
+    a_done, c_done = _bypass_run(bypass_ms=60000.0)
+    assert c_done < a_done  # C ran beside A, before B
+    a_done, c_done = _bypass_run(bypass_ms=0.0)
+    assert c_done > a_done  # C waited for B, which waited for A
+
+
+@pytest.mark.gpu
+def test_mixed_lattices_share_a_batch_and_match_alone():
+    """Requests of different lattices and level counts in one batch give what
+    each gives alone."""
+    q = WloopParms(msl=2, nss=[1, 2], mwlt=2, mwlr=2, op_smear=APE, alpha_ape=0.5, proj_iter=4)
+    reqs = [((8, 4, 4, 4), 3, P, 21), ((6, 4, 6, 4), 0, q, 22), ((12, 6, 6, 6), 3, P, 23)]
+    with Server(max_inflight=1, max_batch=8) as s:
+        s.set_limits(bypass_ms=0.0)
+        ids = [s.submit(n, bc, p, "mixed", seed=sd, eps=0.3) for n, bc, p, sd in reqs]
+        outs = [s.wait(i) for i in ids]
+    assert max(bs for _, _, bs in outs) > 1
+    for (n, bc, p, sd), (res, _, _) in zip(reqs, outs):
+        with Context(n, bc, "mixed") as c:
+            c.generate(sd, 0.3)
+            assert np.array_equal(c.measure(p), res)

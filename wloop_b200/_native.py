@@ -124,6 +124,7 @@ def _load():
         "wlg_server_stats": (i, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                  C.POINTER(C.c_longlong), dp, dp, dp]),
         "wlg_server_budget": (C.c_longlong, [vp]),
+        "wlg_server_set_limits": (i, [vp, C.c_longlong, d]),
         "wlg_dat_error": (C.c_char_p, []),
         "wlg_dat_head": (i, [C.POINTER(WlgParms), i, ip]),
         "wlg_dat_write_head": (i, [C.c_char_p, ip]),
@@ -137,6 +138,10 @@ def _load():
         "wlg_cnfg_read_head": (i, [C.c_char_p, ip, dp]),
         "wlg_cnfg_import": (i, [C.c_char_p, ip, dp, dp]),
         "wlg_cnfg_export": (i, [C.c_char_p, ip, dp, d]),
+        "wlg_import_cnfg": (i, [vp, C.c_char_p, dp]),
+        "wlg_export_cnfg": (i, [vp, C.c_char_p, dp]),
+        "wlg_par_write_bc": (i, [C.c_char_p, i]),
+        "wlg_par_check_bc": (i, [C.c_char_p, C.c_longlong, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

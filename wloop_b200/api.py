@@ -11,6 +11,7 @@ Link fields on the host are numpy complex128 arrays of shape (V, 4, 3, 3)
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 
@@ -192,6 +193,27 @@ class Context:
     def hyp_spatial_links(self, a1, a2, proj=1, piter=4, nsweeps=1, keep=0):
         check(lib.wlg_hyp_spatial(self._h, a1, a2, proj, piter, nsweeps, keep), "hyp_spatial_links")
 
+    # -- configurations in openQCD's exported format ---------------------------
+    def import_cnfg(self, path: str) -> float:
+        """ms10's import_cnfg (main/ms10.c:709-718) into this context: the
+        field of an exported file, with its stored average plaquette checked
+        against the FP64 plaquette of the links read; returns that value."""
+        out = np.zeros(1)
+        check(lib.wlg_import_cnfg(self._h, os.fsencode(path), dptr(out)), "import_cnfg")
+        return float(out[0])
+
+    def export_cnfg(self, path: str) -> float:
+        """Writes the context's field in the exported format with its average
+        plaquette in the head; returns that value."""
+        out = np.zeros(1)
+        check(lib.wlg_export_cnfg(self._h, os.fsencode(path), dptr(out)), "export_cnfg")
+        return float(out[0])
+
+    def average_plaquette(self) -> float:
+        """lnk_plaq_sum over the number of plaquettes: 6 V, or (6 N0 - 3)
+        N1 N2 N3 with open boundary conditions."""
+        return self.lnk_plaq_sum() / plaquette_count(self.n, self.bc)
+
     # -- lnk -------------------------------------------------------------------
     def lnk_plaq_sum(self) -> float:
         out = np.zeros(1)
@@ -271,13 +293,24 @@ class Context:
         check(lib.wlg_restore(self._h), "restore")
 
 
+def plaquette_count(n, bc: int) -> float:
+    """Plaquettes lnk_plaq_sum runs over: 6 V, or (6 N0 - 3) N1 N2 N3 with open
+    boundary conditions (the time plaquettes of the last slice are absent,
+    lnkplaq.c:88)."""
+    vs = float(n[1] * n[2] * n[3])
+    return (6.0 * n[0] - 3.0 if bc == 0 else 6.0 * n[0]) * vs
+
+
 def launch_count() -> int:
     return lib.wlg_launch_count()
 
 
 def peak_tflops(precision: str = "mixed", device: int = 0) -> float:
+    """Measured vector FMA peak: "fp64", "mixed" (scalar FP32 FMAs) or
+    "f32x2" (packed two-lane FP32 FMAs)."""
     out = np.zeros(1)
-    check(lib.wlg_peak_flops(PRECISIONS[precision], device, dptr(out)), "peak_flops")
+    code = 2 if precision == "f32x2" else PRECISIONS[precision]
+    check(lib.wlg_peak_flops(code, device, dptr(out)), "peak_flops")
     return float(out[0])
 
 
@@ -415,6 +448,12 @@ class Server:
     @property
     def budget(self) -> int:
         return int(lib.wlg_server_budget(self._h))
+
+    def set_limits(self, budget_bytes: int = 0, bypass_ms: float = -1.0) -> None:
+        """Memory budget in bytes (> 0 replaces it) and the time the head of
+        the queue may be bypassed by later requests that fit (>= 0)."""
+        check(lib.wlg_server_set_limits(self._h, int(budget_bytes), float(bypass_ms)),
+              "server_set_limits")
 
     def submit(self, n, bc: int, p: WloopParms, precision: str = "mixed", seed: int = 0,
                eps: float = 0.2, links: Optional[np.ndarray] = None) -> int:

@@ -1,9 +1,12 @@
 // ctx.cu -- the C ABI (include/wloop_b200.h): a context owns one lattice on
 // one GPU, its scratch buffers and its stream, and sequences the kernels of
 // smear.cu / loops.cu / layout.cu.
+#include <float.h>
+#include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
+#include <algorithm>
 #include <atomic>
 #include <map>
 #include <string>
@@ -732,6 +735,84 @@ int wlg_plaq_sum(wlg_ctx* c, double* out) {
   return finish("plaq_sum");
 }
 
+// Number of plaquettes the sum runs over: 6 V, or (6 N0 - 3) N1 N2 N3 with
+// open boundary conditions (the time plaquettes of the last slice are
+// absent; lnkplaq.c:88).
+static double plaquette_count(const wlg_ctx* c) {
+  const double vs = (double)c->g.n[1] * c->g.n[2] * c->g.n[3];
+  return (c->bc == 0 ? 6.0 * c->g.n[0] - 3.0 : 6.0 * c->g.n[0]) * vs;
+}
+
+// FP64 average plaquette of the su3_dble field in the staging buffer (the
+// field as uploaded, before any rounding to the context's precision).
+static int staged_average_plaquette(wlg_ctx* c, double* avg) {
+  if (ensure(c->plaq_part, sizeof(double) * std::max(plaq_partials(),
+                                                     plaq_aos_partials(c->g.vol))) ||
+      ensure(c->plaq_out, sizeof(double) * WLG_MAX_SM_LEVELS))
+    return -1;
+  plaq_sum_aos(c->g, c->bc, (const double*)c->staging.p, (double*)c->plaq_part.p,
+               (double*)c->plaq_out.p, c->st);
+  double sum = 0.0;
+  WLG_CUDA(cudaMemcpyAsync(&sum, c->plaq_out.p, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  WLG_CUDA(cudaStreamSynchronize(c->st));
+  *avg = sum / plaquette_count(c);
+  return 0;
+}
+
+int wlg_import_cnfg(wlg_ctx* c, const char* path, double* plaq) {
+  CTX_BEGIN(c);
+  if (!path) {
+    set_error("import_cnfg: null path");
+    return -1;
+  }
+  std::vector<double> host((size_t)4 * 18 * c->g.vol);
+  double stored = 0.0;
+  if (wlg_cnfg_import(path, c->g.n, host.data(), &stored)) {
+    set_error("%s", wlg_cnfg_error());
+    return -1;
+  }
+  if (c->bc == 0) {
+    // set_bc(): the time links of the last slice are zero with open bc
+    const long long vs = (long long)c->g.n[1] * c->g.n[2] * c->g.n[3];
+    for (long long s = (long long)(c->g.n[0] - 1) * vs; s < (long long)c->g.n[0] * vs; s++)
+      memset(host.data() + 18 * (4 * s), 0, 18 * sizeof(double));
+  }
+  if (wlg_upload_links(c, host.data())) return -1;
+  double avg = 0.0;
+  if (staged_average_plaquette(c, &avg)) return -1;
+  // openQCD's import check: |plaq(field) - plaq(head)| <= sqrt(nplaq) DBL_EPSILON
+  const double tol = sqrt(plaquette_count(c)) * DBL_EPSILON;
+  if (plaq) *plaq = avg;
+  if (!(fabs(avg - stored) <= tol)) {
+    set_error("import_cnfg: Incorrect average plaquette in %s (head %.16e, field %.16e)", path,
+              stored, avg);
+    return -1;
+  }
+  return finish("import_cnfg");
+}
+
+int wlg_export_cnfg(wlg_ctx* c, const char* path, double* plaq) {
+  CTX_BEGIN(c);
+  if (!path) {
+    set_error("export_cnfg: null path");
+    return -1;
+  }
+  std::vector<double> host((size_t)4 * 18 * c->g.vol);
+  if (wlg_download_links(c, host.data())) return -1;
+  // the plaquette of exactly the links written, in FP64
+  size_t bytes = host.size() * sizeof(double);
+  if (ensure(c->staging, bytes)) return -1;
+  WLG_CUDA(cudaMemcpyAsync(c->staging.p, host.data(), bytes, cudaMemcpyHostToDevice, c->st));
+  double avg = 0.0;
+  if (staged_average_plaquette(c, &avg)) return -1;
+  if (plaq) *plaq = avg;
+  if (wlg_cnfg_export(path, c->g.n, host.data(), avg)) {
+    set_error("%s", wlg_cnfg_error());
+    return -1;
+  }
+  return finish("export_cnfg");
+}
+
 int wlg_wloop_sum(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat, double* plaq) {
   CTX_BEGIN(c);
   return c->prec == WLG_FP64 ? do_wloop_sum<double>(c, p, wl_mat, plaq)
@@ -1019,7 +1100,24 @@ __global__ void __launch_bounds__(256) k_peak(T* out, int iters, T a, T b) {
   if (s == (T)-12345.0) out[threadIdx.x] = s;  // keeps the chains live
 }
 
-template <class T> static int peak_impl(int device, double* tflops) {
+// the same with packed two-lane FP32 FMAs (fma.rn.f32x2): 8 chains of
+// float2, 16 FMAs per iteration and thread
+__global__ void __launch_bounds__(256) k_peak_x2(float* out, int iters, float a, float b) {
+  float2 x[8];
+  const float2 a2 = make_float2(a, a), b2 = make_float2(b, b);
+#pragma unroll
+  for (int j = 0; j < 8; j++) x[j] = make_float2((threadIdx.x + j) * 1e-3f, (threadIdx.x - j) * 1e-3f);
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) x[j] = __ffma2_rn(x[j], a2, b2);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int j = 0; j < 8; j++) s += x[j].x + x[j].y;
+  if (s == -12345.0f) out[threadIdx.x] = s;  // keeps the chains live
+}
+
+template <class T> static int peak_impl(int device, double* tflops, bool packed = false) {
   WLG_CUDA(cudaSetDevice(device));
   T* out = nullptr;
   WLG_CUDA(cudaMalloc(&out, 256 * sizeof(T)));
@@ -1030,7 +1128,10 @@ template <class T> static int peak_impl(int device, double* tflops) {
   float best = 1e30f;
   for (int rep = 0; rep < 4; rep++) {
     cudaEventRecord(a);
-    k_peak<T><<<blocks, 256>>>(out, iters, (T)0.999, (T)1e-4);
+    if (packed)
+      k_peak_x2<<<blocks, 256>>>((float*)out, iters, 0.999f, 1e-4f);
+    else
+      k_peak<T><<<blocks, 256>>>(out, iters, (T)0.999, (T)1e-4);
     cudaEventRecord(b);
     cudaEventSynchronize(b);
     float ms = 0;
@@ -1040,7 +1141,7 @@ template <class T> static int peak_impl(int device, double* tflops) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   cudaFree(out);
-  double flops = 2.0 * 8.0 * iters * 256.0 * blocks;
+  double flops = 2.0 * (packed ? 16.0 : 8.0) * iters * 256.0 * blocks;
   *tflops = flops / (best * 1e-3) / 1e12;
   return finish("peak_flops");
 }
@@ -1051,5 +1152,6 @@ extern "C" int wlg_peak_flops(int precision, int device, double* tflops) {
     set_error("no CUDA device");
     return -1;
   }
+  if (precision == WLG_PEAK_F32X2) return peak_impl<float>(device, tflops, true);
   return precision == WLG_FP64 ? peak_impl<double>(device, tflops) : peak_impl<float>(device, tflops);
 }

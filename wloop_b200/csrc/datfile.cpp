@@ -6,8 +6,15 @@
 // host byte order (ms10 swaps on big-endian hosts).
 // .par, wloop part (wloop_parms.c:343-382): msl+4 int32 {nss[0..msl-1], mwlt,
 // mwlr, op_smear, proj_iter} then 6 doubles {alpha_ape, alpha_hyp[0..1],
-// alpha_action[0..2]}.  The boundary-condition block that precedes it in a
-// full .par file belongs to openQCD and is not written here.
+// alpha_action[0..2]}.
+// .par, boundary-condition part, which precedes the wloop part (ms10 calls
+// openQCD-1.4's write_bc_parms / check_bc_parms first, main/ms10.c:290-295):
+// one int32 bc type then 10 doubles {cG, cG', cF, cF', phi[0..2],
+// phi'[0..2]}.  ms10 passes cG = cG' = cF = cF' = 1 (ms10.c:290), and the
+// phi angles are zero for open (0) and periodic (3) boundary conditions, the
+// two types this library measures.  openQCD's flags/lat_parms.c is not
+// vendored with the reference: the record is restated from openQCD-1.4's
+// published parameter-file format and is not pinned by any file here.
 #include <stdarg.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -189,6 +196,51 @@ int wlg_par_write_wloop(const char* path, const wlg_wloop_parms* p) {
   size_t iw = fwrite(istd, sizeof(int32_t), p->msl + 4, f.f);
   iw += fwrite(dstd, sizeof(double), 6, f.f);
   if (iw != (size_t)p->msl + 10) return fail("write_wloop_parms: Incorrect write count");
+  return 0;
+}
+
+namespace {
+// the bc record's values for open / periodic boundary conditions
+void bc_record(int bc, int32_t* istd, double dstd[10]) {
+  *istd = bc;
+  const double v[10] = {1.0, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  memcpy(dstd, v, sizeof(v));
+}
+}  // namespace
+
+int wlg_par_write_bc(const char* path, int bc) {
+  if (!path) return fail("wlg_par_write_bc: null argument");
+  if (bc != 0 && bc != 3) return fail("write_bc_parms: only open (0) and periodic (3) boundary conditions");
+  int32_t istd;
+  double dstd[10];
+  bc_record(bc, &istd, dstd);
+  to_le(&istd, 1);
+  to_le(dstd, 10);
+  File f(path, "ab");
+  if (!f.f) return fail("write_bc_parms: unable to open %s", path);
+  size_t iw = fwrite(&istd, sizeof(int32_t), 1, f.f);
+  iw += fwrite(dstd, sizeof(double), 10, f.f);
+  if (iw != 11) return fail("write_bc_parms: Incorrect write count");
+  return 0;
+}
+
+int wlg_par_check_bc(const char* path, long long offset, int bc) {
+  if (!path || offset < 0) return fail("wlg_par_check_bc: null argument");
+  if (bc != 0 && bc != 3) return fail("check_bc_parms: only open (0) and periodic (3) boundary conditions");
+  File f(path, "rb");
+  if (!f.f) return fail("check_bc_parms: unable to open %s", path);
+  if (fseek(f.f, offset, SEEK_SET) != 0) return fail("check_bc_parms: seek failed");
+  int32_t istd, want_i;
+  double dstd[10], want_d[10];
+  size_t ir = fread(&istd, sizeof(int32_t), 1, f.f);
+  ir += fread(dstd, sizeof(double), 10, f.f);
+  if (ir != 11) return fail("check_bc_parms: Incorrect read count");
+  to_le(&istd, 1);
+  to_le(dstd, 10);
+  bc_record(bc, &want_i, want_d);
+  int ie = istd != want_i;
+  for (int i = 0; i < 10; i++) ie |= dstd[i] != want_d[i];
+  if (ie) return fail("check_bc_parms: Parameters do not match");
   return 0;
 }
 

@@ -71,6 +71,12 @@ void project_batch(double* m, int n, int iter, cudaStream_t st);
 template <class T>
 void plaq_sum(const Geo& g, int bc, Links<T> U, double* partial, double* out, cudaStream_t st);
 int plaq_partials();
+// FP64 plaquette sum of a field in device memory in the AoS lexicographic
+// su3_dble layout of the host (noalloc.cu); partials must hold
+// plaq_aos_partials(vol) doubles, out one double (both device memory).
+void plaq_sum_aos(const Geo& g, int bc, const double* links, double* partials, double* out,
+                  cudaStream_t st);
+int plaq_aos_partials(long long vol);
 
 // ---- loops (loops.cu) -----------------------------------------------------
 // lines_dst[sl][k] = lines_src[sl][k](x) * level[sl][k](x + (R-1) k)

@@ -128,6 +128,19 @@ int device_accessible(const void* p, const char* what, int dev) {
 }
 
 }  // namespace
+
+int plaq_aos_partials(long long vol) { return (int)((vol + kChunk - 1) / kChunk); }
+
+void plaq_sum_aos(const Geo& g, int bc, const double* links, double* partials, double* out,
+                  cudaStream_t st) {
+  const int nchunks = plaq_aos_partials(g.vol);
+  k_plaq_chunks<<<nchunks, kThreads, 0, st>>>(g, bc, reinterpret_cast<const double2*>(links),
+                                               partials);
+  WLG_LAUNCH_CHECK("plaq_chunks");
+  k_plaq_chunks_total<<<1, kThreads, 0, st>>>(partials, nchunks, out);
+  WLG_LAUNCH_CHECK("plaq_chunks_total");
+}
+
 }  // namespace wlg
 
 using namespace wlg;
@@ -179,14 +192,7 @@ extern "C" int wlg_plaq_sum_noalloc(const double* links, const int n[4], int bc,
     }
     partials = g_partials_addr[dev];
   }
-  Geo g = make_geo(n);
-  const int nchunks = (int)((vol + kChunk - 1) / kChunk);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  k_plaq_chunks<<<nchunks, kThreads, 0, st>>>(g, bc, reinterpret_cast<const double2*>(links),
-                                               partials);
-  WLG_LAUNCH_CHECK("plaq_chunks");
-  k_plaq_chunks_total<<<1, kThreads, 0, st>>>(partials, nchunks, out);
-  WLG_LAUNCH_CHECK("plaq_chunks_total");
+  plaq_sum_aos(make_geo(n), bc, links, partials, out, static_cast<cudaStream_t>(stream));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_error("wlg_plaq_sum_noalloc: %s", cudaGetErrorString(e));

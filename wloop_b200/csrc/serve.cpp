@@ -5,14 +5,21 @@
 // Requests (a lattice, its boundary condition, the loop parameters, the
 // precision, and either a host gauge field or a synthetic-field seed) enter a
 // FIFO queue.  max_inflight worker threads each repeatedly take the oldest
-// pending request together with further pending requests of the same lattice
-// and precision (up to max_batch), as long as their device footprint fits both
-// the server's memory budget (a fraction of the HBM free at start, counting
-// the batch pool's idle memory, minus what the batches in flight reserve) and what cudaMemGetInfo reports free now.
-// The group becomes one wlg_batch on the worker's own stream: requests that
-// arrive while others run are admitted as soon as a worker and memory free up,
-// and the batches of different workers overlap on the device.  Each request's
-// latency is measured from submission to the moment its result is on the host.
+// pending request that fits, together with further pending requests of the
+// same precision (any lattices and loop parameters; up to max_batch), as long
+// as their device footprint fits both the server's memory budget (a fraction
+// of the HBM free at start, counting the batch pool's idle memory, minus what
+// the batches in flight reserve) and what cudaMemGetInfo reports free now.
+// A request at the head of the queue that does not fit yet does not block
+// the ones behind it: later requests that fit are admitted around it, until
+// the head has waited longer than the bypass limit; from then on nothing
+// else starts until the head has started, so a large request cannot starve.
+// The group becomes one wlg_batch on the worker's own stream (a batch holds
+// lattices of any sizes, each measured exactly as it would be alone):
+// requests that arrive while others run are admitted as soon as a worker and
+// memory free up, and the batches of different workers overlap on the
+// device.  Each request's latency is measured from submission to the moment
+// its result is on the host.
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -57,6 +64,7 @@ struct wlg_server {
   long long budget = 0;
   long long reserved = 0;
   int max_batch = 8;
+  double bypass_ms = 5000.0;  // how long the head of the queue may be bypassed
   std::vector<std::thread> workers;
   std::mutex m;
   std::condition_variable cv_work, cv_done;
@@ -75,10 +83,8 @@ long long footprint(const wlg_request& r) {
   return wlg_batch_estimate_bytes(1, r.n, &r.bc, &r.parms, r.precision);
 }
 
-bool same_shape(const wlg_request& a, const wlg_request& b) {
-  return memcmp(a.n, b.n, sizeof(a.n)) == 0 && a.precision == b.precision &&
-         a.parms.msl == b.parms.msl;
-}
+// requests that can share one batch: a batch has one precision
+bool batchable(const wlg_request& a, const wlg_request& b) { return a.precision == b.precision; }
 
 void fail_locked(wlg_server* s, Req* q, const std::string& msg) {
   q->state = 3;
@@ -100,43 +106,66 @@ void worker(wlg_server* s) {
         s->cv_work.wait(lk);
         continue;
       }
-      Req* head = s->reqs[s->pending.front()];
-      if (head->bytes > s->budget) {
-        s->pending.pop_front();
-        char buf[160];
-        snprintf(buf, sizeof(buf), "request needs %.2f GB, more than the server budget %.2f GB",
-                 head->bytes / 1e9, s->budget / 1e9);
-        fail_locked(s, head, buf);
-        s->cv_done.notify_all();
-        continue;
+      // requests that can never fit the budget fail at once, wherever they are
+      bool failed_one = false;
+      for (auto it = s->pending.begin(); it != s->pending.end();) {
+        Req* q = s->reqs[*it];
+        if (q->bytes > s->budget) {
+          char buf[160];
+          snprintf(buf, sizeof(buf), "request needs %.2f GB, more than the server budget %.2f GB",
+                   q->bytes / 1e9, s->budget / 1e9);
+          fail_locked(s, q, buf);
+          it = s->pending.erase(it);
+          failed_one = true;
+        } else {
+          ++it;
+        }
       }
+      if (failed_one) s->cv_done.notify_all();
+      if (s->pending.empty()) continue;
+      Req* head = s->reqs[s->pending.front()];
       size_t fr0 = 0, tot = 0;
       cudaMemGetInfo(&fr0, &tot);
       // free for a batch: the device's free memory plus what the batch pool
       // keeps idle from earlier batches
       const long long fr = (long long)fr0 + wlg_batch_pool_idle_bytes(s->dev);
-      if (s->reserved + head->bytes > s->budget || fr < head->bytes) {
-        if (s->reserved == 0 && fr < head->bytes) {
-          // nothing of ours is in flight: the device is full for other reasons
-          s->pending.pop_front();
-          fail_locked(s, head, "not enough free device memory");
-          s->cv_done.notify_all();
-          continue;
-        }
-        s->cv_work.wait(lk);  // wait for a batch in flight to release memory
+      auto fits = [&](const Req* q, long long extra) {
+        return s->reserved + extra + q->bytes <= s->budget && extra + q->bytes <= fr;
+      };
+      if (!fits(head, 0) && s->reserved == 0 && fr < head->bytes) {
+        // nothing of ours is in flight: the device is full for other reasons
+        s->pending.pop_front();
+        fail_locked(s, head, "not enough free device memory");
+        s->cv_done.notify_all();
         continue;
       }
-      for (auto it = s->pending.begin(); it != s->pending.end() && (int)group.size() < s->max_batch;) {
+      // the oldest request that fits; the head is bypassed only while it has
+      // waited less than the bypass limit
+      const bool head_may_wait = now_ms() - head->t_submit < s->bypass_ms;
+      auto first = s->pending.end();
+      for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
+        if (fits(s->reqs[*it], 0)) {
+          first = it;
+          break;
+        }
+        if (!head_may_wait) break;  // only the head may start now
+      }
+      if (first == s->pending.end()) {
+        // wait for a batch in flight to release memory (or for the head's
+        // bypass window to close)
+        s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+        continue;
+      }
+      for (auto it = first; it != s->pending.end() && (int)group.size() < s->max_batch;) {
         Req* q = s->reqs[*it];
-        if (group.empty() || (same_shape(group[0]->r, q->r) &&
-                              s->reserved + need + q->bytes <= s->budget &&
-                              need + q->bytes <= fr)) {
+        if (group.empty() || (batchable(group[0]->r, q->r) && fits(q, need))) {
           group.push_back(q);
           need += q->bytes;
           it = s->pending.erase(it);
         } else {
           ++it;
         }
+        if (!head_may_wait) break;  // a starving head starts alone
       }
     }
     s->reserved += need;
@@ -331,5 +360,14 @@ int wlg_server_stats(wlg_server* s, long long* completed, long long* failed, lon
 }
 
 long long wlg_server_budget(wlg_server* s) { return s ? s->budget : -1; }
+
+int wlg_server_set_limits(wlg_server* s, long long budget_bytes, double bypass_ms) {
+  if (!s) return -1;
+  std::lock_guard<std::mutex> lk(s->m);
+  if (budget_bytes > 0) s->budget = budget_bytes;
+  if (bypass_ms >= 0.0) s->bypass_ms = bypass_ms;
+  s->cv_work.notify_all();
+  return 0;
+}
 
 }  // extern "C"

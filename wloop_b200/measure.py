@@ -4,19 +4,26 @@ ms10 (main/ms10.c:687-760) visits the configurations first, first+step, ...,
 last; for each it HYP-smears the gauge field with alpha_action and computes
 the Wilson-loop matrices (set_data, ms10.c:633-646), then appends one record
 to its .dat file (save_data, ms10.c:649-659).  `run` does the same on the GPU
-through the C ABI and writes the same .dat format (head and records through
-wlg_dat_* of libwloop_b200.so) plus the wloop part of the .par file.
+through the C ABI and writes ms10's files under ms10's names
+(ms10.c:254-256): <name>.ms10.dat (head and records through wlg_dat_* of
+libwloop_b200.so), <name>.ms10.par (the boundary-condition record, then the
+wloop record, in the order ms10 writes them, ms10.c:290-313) and a log
+<name>.ms10.log.  The log adds, per configuration, the average plaquette
+after the HYP smearing and after every smearing level (lnk_plaq_sum,
+lnkplaq.c:117-128, over the number of plaquettes), a diagnostic ms10 itself
+does not print (its print_log is commented out, ms10.c:722).
 
 Several processes (one per GPU, launched by torchrun) share a run as
 replicas: rank r measures every world-th configuration into its own file
-<name>.r<rank>.dat, and `merge` interleaves those into the single
-<name>.dat ordered by configuration number that one process would have
+<name>.ms10.r<rank>.dat, and `merge` interleaves those into the single
+<name>.ms10.dat ordered by configuration number that one process would have
 written.  No device data crosses ranks.
 
-Configurations come from a callable nc -> host field (complex128, shape
-(V, 4, 3, 3), su3_dble layout) -- `cnfg_source` reads ms10's exported files
-<cnfg_dir>/<name>n<nc> -- or, without one, are synthetic fields generated on
-the device with seed nc.
+Configurations come from ms10's exported files <cnfg_dir>/<name>n<nc>
+(imported into the context with the stored plaquette checked, as openQCD's
+import_cnfg does), from a callable nc -> host field (complex128, shape
+(V, 4, 3, 3), su3_dble layout), or, without either, are synthetic fields
+generated on the device with seed nc.
 """
 from __future__ import annotations
 
@@ -29,7 +36,7 @@ from typing import Callable, List, Optional, Sequence, Tuple
 import numpy as np
 
 from ._native import WlgError, dptr, iptr, lib
-from .api import Context, WloopParms
+from .api import Context, WloopParms, plaquette_count
 from .replicas import Replicas, config_numbers, shard
 
 
@@ -110,13 +117,25 @@ def merge(parts: Sequence[str], out: str) -> int:
     return len(recs)
 
 
-def write_par(path: str, p: WloopParms) -> None:
-    """Appends the wloop record of the .par file (wloop_parms.c:343-382)."""
+BC_RECORD_BYTES = 4 + 8 * 10
+
+
+def write_par(path: str, p: WloopParms, bc: Optional[int] = None) -> None:
+    """Appends the .par records: with bc given, the boundary-condition record
+    first (write_bc_parms, ms10.c:295), then the wloop record
+    (write_wloop_parms, wloop_parms.c:343-382)."""
+    if bc is not None:
+        _check(lib.wlg_par_write_bc(_b(path), int(bc)), "write_bc_parms")
     cp = p.to_c()
     _check(lib.wlg_par_write_wloop(_b(path), C.byref(cp)), "write_wloop_parms")
 
 
-def check_par(path: str, p: WloopParms, offset: int = 0) -> None:
+def check_par(path: str, p: WloopParms, offset: int = 0, bc: Optional[int] = None) -> None:
+    """Compares a .par file with the run's parameters: with bc given, the
+    boundary-condition record at `offset`, then the wloop record after it."""
+    if bc is not None:
+        _check(lib.wlg_par_check_bc(_b(path), offset, int(bc)), "check_bc_parms")
+        offset += BC_RECORD_BYTES
     cp = p.to_c()
     _check(lib.wlg_par_check_wloop(_b(path), offset, C.byref(cp)), "check_wloop_parms")
 
@@ -189,19 +208,36 @@ class Run:
 
 def dat_path(out_dir: str, name: str, rank: int = 0, world: int = 1) -> str:
     if world == 1:
-        return os.path.join(out_dir, f"{name}.dat")
-    return os.path.join(out_dir, f"{name}.r{rank}.dat")
+        return os.path.join(out_dir, f"{name}.ms10.dat")
+    return os.path.join(out_dir, f"{name}.ms10.r{rank}.dat")
 
 
-def _device_measure(run: Run, source, device: int):
+def par_path(out_dir: str, name: str) -> str:
+    return os.path.join(out_dir, f"{name}.ms10.par")
+
+
+def log_path(out_dir: str, name: str) -> str:
+    return os.path.join(out_dir, f"{name}.ms10.log")
+
+
+def _device_measure(run: Run, source, device: int, cnfg_dir: Optional[str] = None):
+    """nc -> (wl_mat, average plaquette after HYP, average plaquette of every
+    level): hyp_links(alpha_action) then wloop_sum, as Context.measure."""
     ctx = Context(run.n, run.bc, run.precision, device=device)
+    p = run.parms
+    nplaq = plaquette_count(run.n, run.bc)
 
-    def measure(nc: int) -> np.ndarray:
-        if source is None:
+    def measure(nc: int):
+        if cnfg_dir is not None:
+            ctx.import_cnfg(os.path.join(cnfg_dir, f"{run.name}n{nc}"))
+        elif source is None:
             ctx.generate(nc, run.eps)
         else:
             ctx.upload(source(nc))
-        return ctx.measure(run.parms)
+        ctx.hyp_links(*p.alpha_action, p.proj, p.proj_iter)
+        plaq_hyp = ctx.lnk_plaq_sum() / nplaq
+        wl, pl = ctx.wloop_sum(p, plaq=True)
+        return wl, plaq_hyp, pl / nplaq
 
     return ctx, measure
 
@@ -209,13 +245,16 @@ def _device_measure(run: Run, source, device: int):
 def run(r: Run, out_dir: str, replicas: Optional[Replicas] = None,
         source: Optional[Callable[[int], np.ndarray]] = None,
         measure: Optional[Callable[[int], np.ndarray]] = None,
-        log: Optional[Callable[[str], None]] = None) -> dict:
+        log: Optional[Callable[[str], None]] = None, cnfg_dir: Optional[str] = None) -> dict:
     """Measures this rank's share of the run's configurations and appends one
     record per configuration to its .dat file.  `measure` (nc -> wl_mat)
     replaces the device measurement; by default a Context on this rank's
-    local GPU runs HYP(alpha_action) + wloop_sum on each configuration.
-    With several replicas, rank 0 merges the per-rank files into
-    <name>.dat after all ranks have finished."""
+    local GPU runs HYP(alpha_action) + wloop_sum on each configuration, on
+    the exported file <cnfg_dir>/<name>n<nc> when cnfg_dir is given.
+    Every rank writes its lines to <name>.ms10.log (rank r > 0 to
+    <name>.ms10.r<rank>.log) and to `log`.  With several replicas, rank 0
+    merges the per-rank files into <name>.ms10.dat after all ranks have
+    finished."""
     rank = replicas.rank if replicas else 0
     world = replicas.world if replicas else 1
     local = replicas.device if replicas else 0
@@ -224,30 +263,50 @@ def run(r: Run, out_dir: str, replicas: Optional[Replicas] = None,
     path = dat_path(out_dir, r.name, rank, world)
     write_head(path, head)
     if rank == 0:
-        par = os.path.join(out_dir, f"{r.name}.par")
+        par = par_path(out_dir, r.name)
         if os.path.exists(par):
             os.remove(par)
-        write_par(par, r.parms)
+        write_par(par, r.parms, r.bc)
+    logfile = log_path(out_dir, r.name) if rank == 0 else \
+        os.path.join(out_dir, f"{r.name}.ms10.r{rank}.log")
+    flog = open(logfile, "w")
+
+    def say(line: str) -> None:
+        flog.write(line + "\n")
+        flog.flush()
+        if log:
+            log(line)
+
     mine = shard(r.configs, rank, world)
     ctx = None
     if measure is None:
-        ctx, measure = _device_measure(r, source, local)
+        ctx, measure = _device_measure(r, source, local, cnfg_dir)
     seconds = []
+    cum = np.cumsum(r.parms.nss[:r.parms.msl])
     try:
         for nc in mine:
             t0 = time.perf_counter()
-            wl = measure(nc)
+            say(f"Configuration no {nc}")
+            res = measure(nc)
+            wl = res[0] if isinstance(res, tuple) else res
             if wl.size != head[0]:
                 raise WlgError(f"measurement of configuration {nc} has {wl.size} entries, "
                                f"expected {head[0]}")
             append(path, nc, wl)
             seconds.append(time.perf_counter() - t0)
-            if log:
-                log(f"Configuration no {nc} fully processed in {seconds[-1]:.2e} sec")
+            if isinstance(res, tuple):
+                say(f"Average plaquette after HYP smearing = {res[1]:.15e}")
+                for sl, v in enumerate(res[2]):
+                    say(f"Average plaquette at smearing level {sl} ({int(cum[sl])} sweeps) = "
+                        f"{v:.15e}")
+            say(f"Configuration no {nc} fully processed in {seconds[-1]:.2e} sec "
+                f"(average = {sum(seconds) / len(seconds):.2e} sec)")
     finally:
+        flog.close()
         if ctx is not None:
             ctx.close()
-    out = {"rank": rank, "world": world, "path": path, "configs": mine, "seconds": seconds}
+    out = {"rank": rank, "world": world, "path": path, "configs": mine, "seconds": seconds,
+           "log": logfile}
     if world > 1:
         replicas.barrier()
         if rank == 0:
@@ -259,7 +318,7 @@ def run(r: Run, out_dir: str, replicas: Optional[Replicas] = None,
                 if have != want:
                     raise WlgError(f"merge: rank {k} wrote {have} of its {want} records "
                                    f"({part}); the merged file is not written")
-            out["merged"] = os.path.join(out_dir, f"{r.name}.dat")
+            out["merged"] = dat_path(out_dir, r.name)
             out["records"] = merge(parts, out["merged"])
         replicas.barrier()
     return out
@@ -299,8 +358,7 @@ def main(argv=None) -> int:
                    a.proj_iter)
     r = Run(a.name, n, a.bc, p, a.first, a.last, a.step, a.precision, a.eps)
     with Replicas() as rep:
-        src = cnfg_source(a.cnfg_dir, a.name, n) if a.cnfg_dir else None
-        res = run(r, a.out, rep, source=src, log=print if rep.rank == 0 else None)
+        res = run(r, a.out, rep, log=print if rep.rank == 0 else None, cnfg_dir=a.cnfg_dir)
     if res.get("merged"):
         print(f"{res['records']} records in {res['merged']}")
     return 0
