@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--skip-fp64", action="store_true", help="do not run the FP64 comparison")
     ap.add_argument("--skip-cpu", action="store_true", help="do not time the CPU baseline")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--forms", default="", help="comma-separated contraction forms to time "
+                    "beside the default (mixed), e.g. 8,9")
     ap.add_argument("--lattice", default=None,
                     help="N0xN1xN2xN3 override for small profiling captures (not a bench line)")
     ap.add_argument("--workload", default="c3", choices=["c3", "c3b", "c4", "c5", "c5sweep"],
@@ -341,8 +343,10 @@ def run_ours(args, rank, world, local):
     p = w.parms
     fl = flops_per_config(w)
 
-    def timed_value(prec, steps, warmup, profile):
+    def timed_value(prec, steps, warmup, profile, variant=0):
         ctx = Context(w.n, w.bc, prec, device=local)
+        if variant:
+            ctx.set_contract_tuning(variant=variant)
         ctx.generate(w.seed + 1000 * rank, w.eps)
         ctx.snapshot()
         for _ in range(warmup):
@@ -428,6 +432,17 @@ def run_ours(args, rank, world, local):
                 "frac_entries_le_1e-6": float(np.mean(rel <= 1e-6)),
                 "median_rel_err": float(np.median(rel)),
                 "contract_ms_per_launch": kt64["contract"][0] / max(1, kt64["contract"][1])}
+
+    # ---- the contraction forms side by side (same run, same clocks) ----
+    forms = None
+    if args.forms and args.precision == "mixed":
+        forms = {}
+        for v in (int(x) for x in args.forms.split(",")):
+            cv, msv, wlv, ktv, _, _ = timed_value("mixed", max(2, min(args.steps, 3)), 1, True, v)
+            cv.close()
+            forms[str(v)] = {"ms_per_step": barrier_max(msv),
+                             "contract_ms_per_launch": ktv["contract"][0] / max(1, ktv["contract"][1]),
+                             "max_abs_diff_vs_default": float(np.abs(wlv - wl_main).max())}
 
     # ---- roofline of the dominant kernel (contraction) ----
     c_ms, c_n = kt["contract"]
@@ -515,6 +530,7 @@ def run_ours(args, rank, world, local):
                 "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
                 "gpu_launches": launches, "fp64_form": fp64, "kernel_share": shares,
                 "mixed_vs_oracle_fixture": vs_oracle, "c1_measured_pair": c1,
+                "contract_forms": forms,
                 "algorithmic_flops_per_config": fl["total"]}
         print(json.dumps(line), flush=True)
     rep.close()

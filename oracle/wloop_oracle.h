@@ -5,11 +5,13 @@
  * compared against; only tests/, __graft_entry__.smoke() and the cpu_baseline
  * leg of bench.py may load it.  The product library never links it.
  *
- * Parity status: the reference (bjoern-leder/wloop) cannot be compiled here
- * (openQCD-1.4 and MPI are absent) and ships no golden vectors.  The oracle is
- * pinned by the reference's own property checks restated in tests/ (unit
- * field, HYP == APE identity, gauge and translation invariance, unitarity
- * after projection), not by stored reference output.
+ * Parity status: pinned to the reference (bjoern-leder/wloop) itself.  Its
+ * modules compile unchanged against the one-process openQCD-1.4 interface in
+ * refshim/ (oracle/Makefile `ref`; openQCD and MPI are not vendored), and
+ * tests/test_reference.py holds this oracle to that build at 1e-13, function
+ * by function and on whole measurements.  The reference's own property checks
+ * (unit field, HYP == APE identity, gauge and translation invariance,
+ * unitarity after projection) are restated in tests/ as well.
  *
  * Field layout: lexicographic sites ix = x3 + N3*(x2 + N2*(x1 + N1*x0))
  * (the index openQCD's ipt[] maps from), 4 links per site, link (ix,mu) at

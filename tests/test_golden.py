@@ -187,3 +187,54 @@ def test_gpu_c4_batch_members_match_fixtures(prec):
                 assert err <= 1e-12
             else:
                 assert rel.max() <= 1e-6
+            rpath = os.path.join(HERE, "ref_" + name)
+            if os.path.exists(rpath):
+                # the same against the reference's own output
+                rf = dict(f, wl=dict(np.load(rpath))["wl"])
+                if prec == "fp64":
+                    assert _check(got, rf, 1e-12) <= 1e-12
+                else:
+                    assert _plain_rel(got, rf).max() <= 1e-6
+
+
+# ---------------------------------------------------------------------------
+# fixtures made by the reference itself (tests/golden/make_ref_golden.py)
+# ---------------------------------------------------------------------------
+REF = ["c2_24x24x24x48_open", "c4_00_16x16x16x32_periodic", "c4_48_24x24x24x48_periodic"]
+
+
+def load_ref(name):
+    path = os.path.join(HERE, "ref_" + name + ".npz")
+    if not os.path.exists(path):
+        pytest.skip(f"no reference fixture ref_{name}.npz")
+    return dict(np.load(path))
+
+
+@pytest.mark.parametrize("name", REF)
+def test_oracle_fixture_matches_reference_fixture(name):
+    """The oracle's full-size fixture against the reference's own output on
+    the same field (same sha256) and time slices."""
+    f, r = load(name + ".npz"), load_ref(name)
+    assert str(r["sha256"]) == str(f["sha256"])
+    assert np.array_equal(r["x0"], f["x0"])
+    assert _check(r["wl"], f, 1e-13) <= 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_gpu_c2_matches_reference_fixture(prec):
+    from wloop_b200 import Context
+    name = "c2_24x24x24x48_open"
+    f, r = load(name + ".npz"), load_ref(name)
+    n, bc, u = field(f)
+    with Context(n, bc, prec) as c:
+        c.upload(u)
+        got = c.measure(parms(f)).reshape(n[0], -1)[f["x0"]]
+    ref = dict(f, wl=r["wl"])  # the reference's W with the oracle's |terms| scale
+    err = _check(got, ref, 1e-12)
+    rel = _plain_rel(got, ref)
+    print(f"{name} {prec} vs reference: max scaled {err:.2e}, max plain relative {rel.max():.2e}")
+    if prec == "fp64":
+        assert err <= 1e-12
+    else:
+        assert rel.max() <= 1e-6

@@ -406,3 +406,25 @@ def test_lines_left_by_the_measurement(prec, form):
                     want = want @ lev[y @ st, k]
                 tol = 1e-13 if prec == "fp64" else 2e-6
                 assert np.max(np.abs(got[:, k] - want)) < tol, (sl, k)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [0, 3, 4])
+def test_ninth_form_matches_default(case):
+    """The ninth contraction form (one 32-column chunk per warp, per-warp
+    partial records) gives the default form's mixed result up to the order of
+    the FP64 sums, and the oracle's within 1e-6 plain relative."""
+    n, bc, p = CASES[case]
+    u = generate_links(n, bc, 700 + case, 0.25)
+    uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
+    ref = O.wloop_sum(n, bc, uh, p)
+    with Context(n, bc, "mixed") as c:
+        c.upload(u)
+        base = c.measure(p)
+        c.set_contract_tuning(variant=9)
+        c.upload(u)
+        got = c.measure(p)
+    nz = ref != 0.0
+    assert np.all(got[~nz] == 0.0)
+    assert np.abs(got - base).max() <= 1e-13 * np.abs(base).max()
+    assert (np.abs(got - ref)[nz] / np.abs(ref)[nz]).max() <= 1e-6

@@ -381,6 +381,13 @@ static int do_loops(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
   ContractPlan cp = contract_plan(g, msl, p->mwlt, c->prec == WLG_FP64, c->cG, c->cNCB, c->cBlock);
   if (c->cVariant) cp.variant = c->cVariant;
   if (c->cSB) cp.SB = c->cSB;
+  if (cp.variant == 9) {
+    if (!contract9_available(msl, cp.G, c->prec == WLG_FP64)) {
+      set_error("contract: the ninth form needs FP32, msl 4-6 and G = (msl+1)/2");
+      return -1;
+    }
+    contract9_plan(cp, g, msl, p->mwlt);
+  }
   c->used_variant = cp.variant;
   size_t nwl = (size_t)msl * msl * p->mwlt * p->mwlr * g.n[0];
   if (ensure(c->partial, sizeof(double) * cp.partial_doubles) || ensure(c->wl, sizeof(double) * nwl))
@@ -975,7 +982,7 @@ int wlg_reset_kernel_times(wlg_ctx* c) {
 
 int wlg_set_contract_tuning(wlg_ctx* c, int variant, int G, int SB, int nCB, int block) {
   CTX_BEGIN(c);
-  if (variant == 1 || variant < 0 || variant > 8 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
+  if (variant == 1 || variant < 0 || variant > 9 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
       nCB < 0 || (block != 0 && (block % 32 != 0 || block > 128)) ||
       (variant == 2 && G == 6 && SB == 2) || (variant >= 3 && G > 4)) {
     set_error("bad contraction tuning (variant %d, G %d, SB %d, nCB %d, block %d)", variant, G,

@@ -104,7 +104,12 @@ template <class T>
 void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
               const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
               const typename V2<T>::t* level, typename V2<T>::t* next, cudaStream_t st);
-inline bool contract_fuses_lines(const ContractPlan& p) { return p.variant >= 4 && p.variant <= 8; }
+inline bool contract_fuses_lines(const ContractPlan& p) { return p.variant >= 4 && p.variant <= 9; }
+// the ninth form (FP32, msl 4-6, G = (msl+1)/2): one 32-column chunk per warp,
+// row sums written to per-warp partial records; contract9_plan turns a plan
+// into one (nCB then counts 32-column chunks)
+bool contract9_available(int msl, int G, bool fp64);
+void contract9_plan(ContractPlan& p, const Geo& g, int msl, int mwlt);
 // the bulk-staged forms need time slices of whole 32-site tiles
 inline bool contract_can_bulk(const Geo& g) { return g.vs % 32 == 0; }
 // 1 if a bulk-staged contraction gave up waiting for its copies since the

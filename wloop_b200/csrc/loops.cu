@@ -826,6 +826,210 @@ __global__ void __launch_bounds__(128, MINB) kb_contract4(const CArgs<T>* __rest
   contract4_body<T, G, MSL, BULK, PK>(A[c], (int)(blockIdx.x - pre[c]));
 }
 
+// ---------------------------------------------------------------------------
+// contraction kernel, ninth form (FP32 only): the eighth form reshaped for
+// four blocks per SM.  Each warp owns one 32-column chunk (no column passes),
+// so it needs no accumulator rows: after every step the lanes that sum a row
+// write it straight into the warp's own partial record in global memory,
+// [x0][group][chunk][T][G][msl] (the reduction kernel sums the records of
+// all chunks).  A staged line takes 72 bytes (four 16-byte copies and one
+// 8-byte copy of its first 36 floats; the 80-byte tile slot ends in 8 bytes
+// of padding) instead of 80, so a 128-thread block holds 55 KB of shared
+// memory instead of 75, and the launch bounds cap the registers at 128.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+
+constexpr int kLv9 = 4 * 512 + 256;  // stage bytes per level and warp
+
+__device__ __forceinline__ void ld_stage9(M3<float>& m, const char* slot, const char* tail) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    float4 v = *reinterpret_cast<const float4*>(slot + q * 512);
+    m.e[2 * q] = make_float2(v.x, v.y);
+    m.e[2 * q + 1] = make_float2(v.z, v.w);
+  }
+  m.e[8] = *reinterpret_cast<const float2*>(tail);
+}
+
+template <int G, int MSL>
+__device__ __forceinline__ void contract9_body(const CArgs<float>& A, int bid) {
+  extern __shared__ double stage9[];  // [nwarps][msl][4 x 512 B + 256 B]
+  static_assert(G >= 1 && G <= 4, "trace rows go to the level's first G chunks");
+  constexpr int msl = MSL;
+  const Geo& g = A.g;
+  const float2* __restrict__ u0 = A.u0;
+  const float2* __restrict__ lines = A.lines;
+  const int mwlt = A.mwlt, R = A.R, ngrp = A.ngrp, nchunk = A.nCB;
+  const int N0 = g.n[0], vs = g.vs, vol = g.vol;
+  int b = bid;
+  const int x0 = b % N0;
+  b /= N0;
+  const int grp = b % ngrp;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int chunk = (b / ngrp) * nwarps + warp;
+  if (chunk >= nchunk) return;  // the whole warp; the kernel has no block barrier
+  char* wst = reinterpret_cast<char*>(stage9) + (size_t)warp * msl * kLv9;
+  char* myslot = wst + lane * 16;
+  char* mytail = wst + 4 * 512 + lane * 8;
+  constexpr int nrows = G * msl;
+  double* __restrict__ out = A.partial + ((size_t)(x0 * ngrp + grp) * nchunk + chunk) * mwlt * nrows;
+
+  const int s1_0 = grp * G;
+  const int ncol = 3 * vs;
+  const int col = chunk * 32 + lane;
+  const bool active = col < ncol;
+  const int cc = active ? col : chunk * 32;
+  const int k = cc / vs, xs = cc - k * vs;
+  int xsR;
+  {
+    const int x1 = xs / g.st[1], r = xs - x1 * g.st[1];
+    const int x2 = r / g.st[2], x3 = r - x2 * g.st[2];
+    const int xk = (k == 0) ? x1 : ((k == 1) ? x2 : x3);
+    const int nk = g.n[k + 1];
+    int y = xk + (R % nk);
+    if (y >= nk) y -= nk;
+    xsR = xs + (y - xk) * g.st[k + 1];
+  }
+  const size_t fstride = link_elems<float>(vol);
+  const float2* lk = lines + (size_t)k * fstride;
+  const size_t lvl = 3 * fstride;
+  M3<float> C[G];
+#pragma unroll
+  for (int gi = 0; gi < G; gi++) {
+    const int s1 = min(s1_0 + gi, msl - 1);
+    ld(C[gi], lk + (size_t)s1 * lvl, vol, x0 * vs + xs);
+    if (!active) zero(C[gi]);  // idle lanes contribute exact zeros
+  }
+  if (A.next) {
+    // the spatial line step of the next R for this thread's own bottom lines
+    // (compute_uk_long, wloop.c:207-258), as in the fourth form
+    const size_t kof = (size_t)k * fstride;
+#pragma unroll
+    for (int gi = 0; gi < G; gi++) {
+      const int s1 = s1_0 + gi;
+      if (active && s1 < msl) {
+        M3<float> lv, nx;
+        ld(lv, A.level + kof + (size_t)s1 * lvl, vol, x0 * vs + xsR);
+        mul(nx, C[gi], lv);
+        st(A.next + kof + (size_t)s1 * lvl, vol, x0 * vs + xs, nx);
+      }
+    }
+  }
+  M3<float> ua, ub;
+  ld(ua, u0, vol, x0 * vs + xs);
+  ld(ub, u0, vol, x0 * vs + xsR);
+  int t0 = x0;
+  for (int tt = 1; tt <= mwlt; tt++) {
+    const int t1 = (t0 + 1 == N0) ? 0 : t0 + 1;  // x0+T mod N0: the top slice
+    const int stop = t1 * vs + xs;
+    __syncwarp();  // the previous step's rows are read before the stage is refilled
+#pragma unroll
+    for (int s2 = 0; s2 < msl; s2++) {
+      const float2* src = lk + (size_t)s2 * lvl;
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        cp_async16(myslot + s2 * kLv9 + q * 512, chunk_ptr<float>(src, stop, q));
+      cp_async8(mytail + s2 * kLv9, chunk_ptr<float>(src, stop, 4));
+    }
+    cp_async_commit();
+    lmul_dag_inplace_x2<G>(C, ua);
+    rmul_inplace_x2<G>(C, ub);
+    t0 = t1;
+    if (tt < mwlt) {
+      ld(ua, u0, vol, t0 * vs + xs);
+      ld(ub, u0, vol, t0 * vs + xsR);
+    }
+    cp_async_wait_all();
+#pragma unroll
+    for (int s2 = 0; s2 < msl; s2++) {
+      M3<float> l;
+      ld_stage9(l, myslot + s2 * kLv9, mytail + s2 * kLv9);
+      __syncwarp();  // every lane holds level s2 before its chunks are overwritten
+#pragma unroll
+      for (int gi = 0; gi < G; gi++) {
+        const int row = gi * msl + s2;
+        double* dst = reinterpret_cast<double*>(wst + s2 * kLv9 + gi * 512 + (row & 7) * 16);
+        dst[lane] = (double)retr_dag(l, C[gi]);
+      }
+    }
+    __syncwarp();
+    if (lane < nrows) {
+      const int row = lane, gi = row / msl, s2 = row - gi * msl;
+      const double2* src =
+          reinterpret_cast<const double2*>(wst + s2 * kLv9 + gi * 512 + (row & 7) * 16);
+      double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const double2 v = src[j];
+        a0 += v.x;
+        a1 += v.y;
+      }
+      out[(size_t)(tt - 1) * nrows + row] = a0 + a1;
+    }
+  }
+}
+
+template <int G, int MSL>
+__global__ void __launch_bounds__(128, 4) k_contract9(CArgs<float> A) {
+  contract9_body<G, MSL>(A, blockIdx.x);
+}
+
+size_t contract9_smem(int block, int msl) { return (size_t)(block / 32) * msl * kLv9; }
+
+template <int G, int MSL>
+static void launch_contract9_m(const Geo& g, const ContractPlan& p, const float2* u0,
+                               const float2* lines, int mwlt, int R, double* partial,
+                               const float2* level, float2* next, cudaStream_t st) {
+  auto kern = k_contract9<G, MSL>;
+  const size_t smem = contract9_smem(p.block, MSL);
+  static size_t smem_set = 48 * 1024;
+  if (smem > smem_set) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_set = smem;
+  }
+  CArgs<float> A{};
+  A.g = g;
+  A.u0 = u0;
+  A.lines = lines;
+  A.msl = MSL;
+  A.mwlt = mwlt;
+  A.R = R;
+  A.ngrp = p.ngrp;
+  A.nCB = p.nCB;
+  A.partial = partial;
+  A.level = level;
+  A.next = next;
+  const int per_block = p.block / 32;
+  kern<<<g.n[0] * p.ngrp * ((p.nCB + per_block - 1) / per_block), p.block, smem, st>>>(A);
+  WLG_LAUNCH_CHECK("contract9");
+}
+
+bool contract9_available(int msl, int G, bool fp64) {
+  return !fp64 && msl >= 4 && msl <= 6 && G == (msl + 1) / 2;
+}
+
+void contract9_plan(ContractPlan& p, const Geo& g, int msl, int mwlt) {
+  p.variant = 9;
+  p.block = 128;
+  p.nCB = (3 * g.vs + 31) / 32;  // one 32-column chunk per warp
+  p.smem = contract9_smem(p.block, msl);
+  p.partial_doubles = (size_t)g.n[0] * p.ngrp * p.nCB * mwlt * p.G * msl;
+}
+
+static void launch_contract9(const Geo& g, const ContractPlan& p, const float2* u0,
+                             const float2* lines, int msl, int mwlt, int R, double* partial,
+                             const float2* level, float2* next, cudaStream_t st) {
+  switch (msl) {
+    case 4: launch_contract9_m<2, 4>(g, p, u0, lines, mwlt, R, partial, level, next, st); return;
+    case 5: launch_contract9_m<3, 5>(g, p, u0, lines, mwlt, R, partial, level, next, st); return;
+    case 6: launch_contract9_m<3, 6>(g, p, u0, lines, mwlt, R, partial, level, next, st); return;
+    default: set_error("contract: the ninth form needs msl 4-6");
+  }
+}
+
 // level counts with their own fully unrolled kernels (the usual 4-6); others
 // run the generic kernel (MSL = 0)
 static inline int msl_variant(int msl) { return (msl >= 4 && msl <= 6) ? msl : 0; }
@@ -941,6 +1145,18 @@ void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
               const typename V2<T>::t* level, typename V2<T>::t* next, cudaStream_t st) {
   if (next && !contract_fuses_lines(p)) {
     set_error("contract: this form does not compute the next lines");
+    return;
+  }
+  if (p.variant == 9) {
+    if constexpr (sizeof(T) == 4) {
+      if (!contract9_available(msl, p.G, false)) {
+        set_error("contract: the ninth form needs FP32, msl 4-6 and G = (msl+1)/2");
+        return;
+      }
+      launch_contract9(g, p, u0, lines, msl, mwlt, R, partial, level, next, st);
+    } else {
+      set_error("contract: the ninth form is FP32 only");
+    }
     return;
   }
   if (p.variant >= 4 && p.variant <= 8) {
