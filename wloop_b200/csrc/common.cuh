@@ -264,6 +264,86 @@ template <class T> __device__ __forceinline__ void mul_ad(M3<T>& c, const M3<T>&
     }
 }
 
+// FP32 single products as packed two-lane FMAs (fma.rn.f32x2): a complex
+// multiply-add c += p q runs as {c.re, c.im} += P1 * {p.re, p.re} + P2 *
+// {p.im, p.im}, with p's entries broadcast into pairs once per product and
+// the pairs P1, P2 of the other factor formed once per entry (q itself and
+// q turned by a quarter, conjugated as the product needs).  The products of
+// the scalar forms above in the same k order.
+__device__ __forceinline__ float2 f2bc(float v) { return make_float2(v, v); }
+
+// c = a*b: a_ik b_kj = {b.re, b.im} a.re + {-b.im, b.re} a.im
+template <> __device__ __forceinline__ void mul<float>(M3<float>& c, const M3<float>& a,
+                                                       const M3<float>& b) {
+  float2 rb[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) rb[k] = make_float2(-b.e[k].y, b.e[k].x);
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const float2 ar0 = f2bc(a.e[3 * i].x), ai0 = f2bc(a.e[3 * i].y);
+    const float2 ar1 = f2bc(a.e[3 * i + 1].x), ai1 = f2bc(a.e[3 * i + 1].y);
+    const float2 ar2 = f2bc(a.e[3 * i + 2].x), ai2 = f2bc(a.e[3 * i + 2].y);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      float2 o = __fmul2_rn(b.e[j], ar0);
+      o = __ffma2_rn(rb[j], ai0, o);
+      o = __ffma2_rn(b.e[3 + j], ar1, o);
+      o = __ffma2_rn(rb[3 + j], ai1, o);
+      o = __ffma2_rn(b.e[6 + j], ar2, o);
+      o = __ffma2_rn(rb[6 + j], ai2, o);
+      c.e[3 * i + j] = o;
+    }
+  }
+}
+
+// c = a^dag*b: conj(a_ki) b_kj = {b.re, b.im} a.re + {b.im, -b.re} a.im
+template <> __device__ __forceinline__ void mul_da<float>(M3<float>& c, const M3<float>& a,
+                                                          const M3<float>& b) {
+  float2 rb[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) rb[k] = make_float2(b.e[k].y, -b.e[k].x);
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const float2 ar0 = f2bc(a.e[i].x), ai0 = f2bc(a.e[i].y);
+    const float2 ar1 = f2bc(a.e[3 + i].x), ai1 = f2bc(a.e[3 + i].y);
+    const float2 ar2 = f2bc(a.e[6 + i].x), ai2 = f2bc(a.e[6 + i].y);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      float2 o = __fmul2_rn(b.e[j], ar0);
+      o = __ffma2_rn(rb[j], ai0, o);
+      o = __ffma2_rn(b.e[3 + j], ar1, o);
+      o = __ffma2_rn(rb[3 + j], ai1, o);
+      o = __ffma2_rn(b.e[6 + j], ar2, o);
+      o = __ffma2_rn(rb[6 + j], ai2, o);
+      c.e[3 * i + j] = o;
+    }
+  }
+}
+
+// c = a*b^dag: a_ik conj(b_jk) = {a.re, a.im} b.re + {a.im, -a.re} b.im
+template <> __device__ __forceinline__ void mul_ad<float>(M3<float>& c, const M3<float>& a,
+                                                          const M3<float>& b) {
+  float2 ra[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) ra[k] = make_float2(a.e[k].y, -a.e[k].x);
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const float2 br0 = f2bc(b.e[3 * j].x), bi0 = f2bc(b.e[3 * j].y);
+    const float2 br1 = f2bc(b.e[3 * j + 1].x), bi1 = f2bc(b.e[3 * j + 1].y);
+    const float2 br2 = f2bc(b.e[3 * j + 2].x), bi2 = f2bc(b.e[3 * j + 2].y);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      float2 o = __fmul2_rn(a.e[3 * i], br0);
+      o = __ffma2_rn(ra[3 * i], bi0, o);
+      o = __ffma2_rn(a.e[3 * i + 1], br1, o);
+      o = __ffma2_rn(ra[3 * i + 1], bi1, o);
+      o = __ffma2_rn(a.e[3 * i + 2], br2, o);
+      o = __ffma2_rn(ra[3 * i + 2], bi2, o);
+      c.e[3 * i + j] = o;
+    }
+  }
+}
+
 // In-place products with 6 temporaries: c <- a^dag c (column by column) and
 // c <- c b (row by row).  Same arithmetic as mul_da / mul.
 template <class T> __device__ __forceinline__ void lmul_dag_inplace(M3<T>& c, const M3<T>& a) {
