@@ -103,18 +103,25 @@ def test_budget_counts_memory_the_batch_pool_keeps():
         assert s.budget >= 0.5 * idle
 
 
+# a request that takes the GPU about a tenth of a second
+BIG_N = (64, 32, 32, 32)
+BIG_P = WloopParms(msl=4, nss=[0, 10, 10, 10], mwlt=8, mwlr=6, op_smear=APE, alpha_ape=0.5,
+                   proj_iter=4)
+
+
 def _bypass_run(bypass_ms):
     """A large request A runs; a second large request B waits at the head of
     the queue (the budget holds one large and two small requests); small
     requests C, D behind B.  Returns the completion times of A and C."""
-    big, small = (32, 16, 16, 16), (8, 4, 4, 4)
+    small = (8, 4, 4, 4)
     with Server(max_inflight=3, max_batch=1) as s:
-        s.set_limits(budget_bytes=estimate_bytes(big, 3, P, "fp64") +
+        s.set_limits(budget_bytes=estimate_bytes(BIG_N, 3, BIG_P, "fp64") +
                      2 * estimate_bytes(small, 3, P, "fp64") + 1024, bypass_ms=bypass_ms)
         done = {}
         t0 = time.perf_counter()
-        ids = {k: (s.submit(n, 3, P, "fp64", seed=k + 1, eps=0.25), time.perf_counter())
-               for k, n in enumerate([big, big, small, small])}
+        ids = {k: (s.submit(n, 3, p, "fp64", seed=k + 1, eps=0.25), time.perf_counter())
+               for k, (n, p) in enumerate([(BIG_N, BIG_P), (BIG_N, BIG_P), (small, P),
+                                           (small, P)])}
         for k, (rid, ts) in ids.items():
             _, lat, _ = s.wait(rid)
             done[k] = ts - t0 + lat * 1e-3
@@ -139,8 +146,10 @@ def test_mixed_lattices_share_a_batch_and_match_alone():
     q = WloopParms(msl=2, nss=[1, 2], mwlt=2, mwlr=2, op_smear=APE, alpha_ape=0.5, proj_iter=4)
     reqs = [((8, 4, 4, 4), 3, P, 21), ((6, 4, 6, 4), 0, q, 22), ((12, 6, 6, 6), 3, P, 23)]
     with Server(max_inflight=1, max_batch=8) as s:
-        s.set_limits(bypass_ms=0.0)
+        # the one worker is busy with a large request while the three queue
+        blocker = s.submit(BIG_N, 3, BIG_P, "mixed", seed=20, eps=0.3)
         ids = [s.submit(n, bc, p, "mixed", seed=sd, eps=0.3) for n, bc, p, sd in reqs]
+        s.wait(blocker)
         outs = [s.wait(i) for i in ids]
     assert max(bs for _, _, bs in outs) > 1
     for (n, bc, p, sd), (res, _, _) in zip(reqs, outs):
