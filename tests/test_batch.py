@@ -151,3 +151,25 @@ def test_batch_shapes_agree(prec, same_msl):
                 scale = np.maximum(np.abs(ref[i]), 1e-3)
                 err = np.max(np.abs(b.result(i) - ref[i]) / scale)
                 assert err < (1e-13 if prec == "fp64" else 1e-6), (G, SB, block, i, err)
+
+
+@pytest.mark.gpu
+def test_tune_context_picks_a_shape_with_the_same_result(tmp_path, monkeypatch):
+    """The single-context tuner (every candidate, the ninth form among them)
+    leaves the context on a shape whose result is the default's up to the
+    order of the FP64 sums."""
+    from wloop_b200 import autotune
+    monkeypatch.setenv("WLG_TUNE_CACHE", str(tmp_path / "tune.json"))
+    n, bc = (8, 8, 8, 8), 3
+    p = WloopParms(msl=4, nss=[0, 1, 1, 1], mwlt=4, mwlr=3, op_smear=APE, alpha_ape=0.5,
+                   proj_iter=4)
+    assert any(SB == 9 for _, SB, _, _ in autotune.candidates(4, False, False))
+    with Context(n, bc, "mixed") as c:
+        c.generate(5, 0.3)
+        c.snapshot()
+        base = c.measure(p)
+        shape = autotune.tune_context(c, p, "mixed", use_cache=False)
+        c.restore()
+        got = c.measure(p)
+    assert shape in autotune.candidates(4, False, False)
+    assert np.abs(got - base).max() <= 1e-6 * np.abs(base).max()

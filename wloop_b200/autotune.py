@@ -67,7 +67,16 @@ def candidates(msl: int, fp64: bool, batched: bool) -> List[Shape]:
         for SB in sbs:
             for block in ((64,) if fp64 else (64, 128)):
                 out.append((G, SB, block, 0))
+    if not batched and not fp64 and 4 <= msl <= 6:
+        # the ninth form (one 32-column chunk per warp, four blocks per SM),
+        # marked SB 9; single contexts only, with its own G and block
+        out.append(((msl + 1) // 2, 9, 128, 0))
     return out
+
+
+def _apply(ctx, shape: Shape) -> None:
+    G, SB, block, nCB = shape
+    ctx.set_contract_tuning(_form(G, SB), G, SB if SB <= 2 else 0, nCB, block)
 
 
 def key_for(precision: str, lattices: Sequence[tuple], parms) -> str:
@@ -85,13 +94,12 @@ def tune_context(ctx, parms, precision: str, reps: int = 1, use_cache: bool = Tr
     restored from a snapshot before every run) and applies the best shape."""
     key = key_for(precision, [ctx.n], parms)
     if use_cache and cached(key):
-        G, SB, block, nCB = cached(key)
-        ctx.set_contract_tuning(_form(G, SB), G, SB, nCB, block)
+        _apply(ctx, cached(key))
         return cached(key)
     ctx.snapshot()
     best, best_t = None, float("inf")
     for (G, SB, block, nCB) in candidates(parms.msl, precision == "fp64", batched=False):
-        ctx.set_contract_tuning(_form(G, SB), G, SB, nCB, block)
+        _apply(ctx, (G, SB, block, nCB))
         ctx.restore()
         ctx.measure(parms)  # warm-up
         ctx.reset_kernel_times()
@@ -104,8 +112,7 @@ def tune_context(ctx, parms, precision: str, reps: int = 1, use_cache: bool = Tr
         t = ms / max(1, n)
         if t < best_t:
             best, best_t = (G, SB, block, nCB), t
-    G, SB, block, nCB = best
-    ctx.set_contract_tuning(_form(G, SB), G, SB, nCB, block)
+    _apply(ctx, best)
     ctx.restore()
     _store(key, best)
     return best
@@ -143,8 +150,11 @@ def tune_batch(batch, reps: int = 1, use_cache: bool = True) -> Shape:
 
 
 def _form(G: int, SB: int) -> int:
-    """kernel form of a context shape: 2 for G = 6, 3 for SB = 1 or 2, and
-    for SB = 0 the library's default fourth-form member (0 = automatic)"""
+    """kernel form of a context shape: 2 for G = 6, 3 for SB = 1 or 2, 9 for
+    SB = 9, and for SB = 0 the library's default fourth-form member (0 =
+    automatic)"""
+    if SB == 9:
+        return 9
     return 2 if G > 4 else (0 if SB == 0 else 3)
 
 
