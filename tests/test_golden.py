@@ -121,6 +121,9 @@ def test_gpu_fp64_matches_fixture(name):
     print(f"{name}: fp64 max scaled error {err:.2e}, max plain relative {rel.max():.2e}, "
           f"entries above 1e-12 plain: {int(np.sum(rel > 1e-12))} of {rel.size}")
     assert err <= 1e-12
+    # the full-size fixtures hold no near-zero W: every entry also within
+    # 1e-12 plain relative
+    assert rel.max() <= 1e-12
     assert np.abs(plaq - f["plaq_levels"]).max() / np.abs(f["plaq_levels"]).max() < 1e-12
 
 
