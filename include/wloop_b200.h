@@ -272,7 +272,9 @@ int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
  * ahead, FP32 contexts only, an FP64 context runs form 5; 9: form 8 with one
  * 32-column chunk per warp, 72-byte line staging and per-warp partial
  * records, for four blocks per SM, FP32 contexts with msl 4-6 and the
- * default G only) and SB top levels per reduction (1 or 2; form 3 only). */
+ * default G only; 10: form 8 with the signs of the packed products in the
+ * shared broadcast pairs, the same result) and SB top levels per reduction
+ * (1 or 2; form 3 only). */
 int wlg_set_contract_tuning(wlg_ctx* ctx, int variant, int G, int SB, int nCB, int block);
 /* The context's CUDA stream (cudaStream_t), for callers that record events. */
 void* wlg_stream(wlg_ctx* ctx);

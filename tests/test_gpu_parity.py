@@ -428,3 +428,19 @@ def test_ninth_form_matches_default(case):
     assert np.all(got[~nz] == 0.0)
     assert np.abs(got - base).max() <= 1e-13 * np.abs(base).max()
     assert (np.abs(got - ref)[nz] / np.abs(ref)[nz]).max() <= 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [0, 4])
+def test_tenth_form_is_the_eighth_bit_for_bit(case):
+    """Form 10 moves the signs of the packed products into the shared
+    broadcast pairs: the same products, so the same result as form 8."""
+    n, bc, p = CASES[case]
+    u = generate_links(n, bc, 710 + case, 0.25)
+    out = []
+    for v in (8, 10):
+        with Context(n, bc, "mixed") as c:
+            c.set_contract_tuning(variant=v)
+            c.upload(u)
+            out.append(c.measure(p))
+    assert np.array_equal(out[0], out[1])

@@ -431,22 +431,28 @@ template <> __device__ __forceinline__ float retr_dag<float>(const M3<float>& a,
 // the same k order; within one k the two products of an imaginary part may be
 // added in the other order (FP32 rounding differences only).
 // ---------------------------------------------------------------------------
+// SW (the tenth form's variant): the sign of the second term moves from the
+// per-matrix turned pair into the shared broadcast pair, {c.im, c.re} *
+// {a.im, -a.im} instead of {c.im, -c.re} * {a.im, a.im}: the same products
+// (a sign is exact), so the same result, with 9 sign flips per product
+// instead of 9 per matrix and product.
 // c[g] <- a^dag c[g]   (conj(a_ki) c_kj = {c.re, c.im} a.re + {c.im, -c.re} a.im)
-template <int G>
+template <int G, bool SW = false>
 __device__ __forceinline__ void lmul_dag_inplace_x2(M3<float> (&c)[G], const M3<float>& a) {
   float2 ar[9], ai[9];
 #pragma unroll
   for (int k = 0; k < 9; k++) {
     ar[k] = make_float2(a.e[k].x, a.e[k].x);
-    ai[k] = make_float2(a.e[k].y, a.e[k].y);
+    ai[k] = SW ? make_float2(a.e[k].y, -a.e[k].y) : make_float2(a.e[k].y, a.e[k].y);
   }
 #pragma unroll
   for (int g = 0; g < G; g++)
 #pragma unroll
     for (int j = 0; j < 3; j++) {
       const float2 x0 = c[g].e[j], x1 = c[g].e[3 + j], x2 = c[g].e[6 + j];
-      const float2 r0 = make_float2(x0.y, -x0.x), r1 = make_float2(x1.y, -x1.x),
-                   r2 = make_float2(x2.y, -x2.x);
+      const float2 r0 = SW ? make_float2(x0.y, x0.x) : make_float2(x0.y, -x0.x),
+                   r1 = SW ? make_float2(x1.y, x1.x) : make_float2(x1.y, -x1.x),
+                   r2 = SW ? make_float2(x2.y, x2.x) : make_float2(x2.y, -x2.x);
 #pragma unroll
       for (int i = 0; i < 3; i++) {
         float2 o = __fmul2_rn(x0, ar[i]);
@@ -460,22 +466,24 @@ __device__ __forceinline__ void lmul_dag_inplace_x2(M3<float> (&c)[G], const M3<
     }
 }
 
-// c[g] <- c[g] b   (c_ik b_kj = {c.re, c.im} b.re + {-c.im, c.re} b.im)
-template <int G>
+// c[g] <- c[g] b   (c_ik b_kj = {c.re, c.im} b.re + {-c.im, c.re} b.im;
+// SW: {c.im, c.re} * {-b.im, b.im})
+template <int G, bool SW = false>
 __device__ __forceinline__ void rmul_inplace_x2(M3<float> (&c)[G], const M3<float>& b) {
   float2 br[9], bi[9];
 #pragma unroll
   for (int k = 0; k < 9; k++) {
     br[k] = make_float2(b.e[k].x, b.e[k].x);
-    bi[k] = make_float2(b.e[k].y, b.e[k].y);
+    bi[k] = SW ? make_float2(-b.e[k].y, b.e[k].y) : make_float2(b.e[k].y, b.e[k].y);
   }
 #pragma unroll
   for (int g = 0; g < G; g++)
 #pragma unroll
     for (int i = 0; i < 3; i++) {
       const float2 x0 = c[g].e[3 * i], x1 = c[g].e[3 * i + 1], x2 = c[g].e[3 * i + 2];
-      const float2 r0 = make_float2(-x0.y, x0.x), r1 = make_float2(-x1.y, x1.x),
-                   r2 = make_float2(-x2.y, x2.x);
+      const float2 r0 = SW ? make_float2(x0.y, x0.x) : make_float2(-x0.y, x0.x),
+                   r1 = SW ? make_float2(x1.y, x1.x) : make_float2(-x1.y, x1.x),
+                   r2 = SW ? make_float2(x2.y, x2.x) : make_float2(-x2.y, x2.x);
 #pragma unroll
       for (int j = 0; j < 3; j++) {
         float2 o = __fmul2_rn(x0, br[j]);

@@ -982,7 +982,7 @@ int wlg_reset_kernel_times(wlg_ctx* c) {
 
 int wlg_set_contract_tuning(wlg_ctx* c, int variant, int G, int SB, int nCB, int block) {
   CTX_BEGIN(c);
-  if (variant == 1 || variant < 0 || variant > 9 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
+  if (variant == 1 || variant < 0 || variant > 10 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
       nCB < 0 || (block != 0 && (block % 32 != 0 || block > 128)) ||
       (variant == 2 && G == 6 && SB == 2) || (variant >= 3 && G > 4)) {
     set_error("bad contraction tuning (variant %d, G %d, SB %d, nCB %d, block %d)", variant, G,

@@ -104,7 +104,7 @@ template <class T>
 void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
               const typename V2<T>::t* lines, int msl, int mwlt, int R, double* partial,
               const typename V2<T>::t* level, typename V2<T>::t* next, cudaStream_t st);
-inline bool contract_fuses_lines(const ContractPlan& p) { return p.variant >= 4 && p.variant <= 9; }
+inline bool contract_fuses_lines(const ContractPlan& p) { return p.variant >= 4 && p.variant <= 10; }
 // the ninth form (FP32, msl 4-6, G = (msl+1)/2): one 32-column chunk per warp,
 // row sums written to per-warp partial records; contract9_plan turns a plan
 // into one (nCB then counts 32-column chunks)

@@ -599,7 +599,7 @@ static void launch_contract3_sb(const Geo& g, const ContractPlan& p, const typen
 // PK (FP32 only), the eighth form: the recursion's products as packed
 // two-lane FMAs (lmul_dag_inplace_x2 / rmul_inplace_x2), and each top level's
 // staged line read from shared memory one level ahead.
-template <class T, int G, int MSL, bool BULK, bool PK = false>
+template <class T, int G, int MSL, bool BULK, int PK = 0>
 __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
   extern __shared__ double acc[];  // [nwarps][mwlt][G][msl] doubles, the line stage, mbarriers
   constexpr int NQ = Chunks<T>::N;
@@ -722,9 +722,9 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
         }
         cp_async_commit();
       }
-      if constexpr (PK && sizeof(T) == 4) {
-        lmul_dag_inplace_x2<G>(C, ua);
-        rmul_inplace_x2<G>(C, ub);
+      if constexpr (PK != 0 && sizeof(T) == 4) {
+        lmul_dag_inplace_x2<G, PK == 2>(C, ua);
+        rmul_inplace_x2<G, PK == 2>(C, ub);
       } else {
 #pragma unroll
         for (int gi = 0; gi < G; gi++) lmul_dag_inplace(C[gi], ua);
@@ -751,7 +751,7 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
       } else {
         cp_async_wait_all();
       }
-      if constexpr (PK && sizeof(T) == 4) {
+      if constexpr (PK != 0 && sizeof(T) == 4) {
         // the next level's staged line is read before this level's barrier
         // (its chunks are overwritten only after its own barrier), so the
         // shared-memory latency overlaps this level's traces
@@ -814,12 +814,12 @@ __device__ __forceinline__ void contract4_body(const CArgs<T>& A, int bid) {
   }
 }
 
-template <class T, int G, int MSL, int MINB, bool BULK, bool PK>
+template <class T, int G, int MSL, int MINB, bool BULK, int PK>
 __global__ void __launch_bounds__(128, MINB) k_contract4(CArgs<T> A) {
   contract4_body<T, G, MSL, BULK, PK>(A, blockIdx.x);
 }
 
-template <class T, int G, int MSL, int MINB, bool BULK, bool PK>
+template <class T, int G, int MSL, int MINB, bool BULK, int PK>
 __global__ void __launch_bounds__(128, MINB) kb_contract4(const CArgs<T>* __restrict__ A,
                                                           const long long* __restrict__ pre, int n) {
   const int c = find_item(pre, n, (long long)blockIdx.x);
@@ -1034,7 +1034,7 @@ static void launch_contract9(const Geo& g, const ContractPlan& p, const float2* 
 // run the generic kernel (MSL = 0)
 static inline int msl_variant(int msl) { return (msl >= 4 && msl <= 6) ? msl : 0; }
 
-template <class T, int G, int MSL, bool BULK, bool PK>
+template <class T, int G, int MSL, bool BULK, int PK>
 static void launch_contract4_m(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
                                const typename V2<T>::t* lines, int msl, int mwlt, int R,
                                double* partial, const typename V2<T>::t* level,
@@ -1064,7 +1064,7 @@ static void launch_contract4_m(const Geo& g, const ContractPlan& p, const typena
 }
 
 // unroll_msl: msl to unroll the level loops for, 0 for the generic kernel
-template <class T, int G, bool BULK, bool PK = false>
+template <class T, int G, bool BULK, int PK = 0>
 static void launch_contract4_b(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
                                const typename V2<T>::t* lines, int msl, int unroll_msl, int mwlt,
                                int R, double* partial, const typename V2<T>::t* level,
@@ -1078,15 +1078,21 @@ static void launch_contract4_b(const Geo& g, const ContractPlan& p, const typena
 }
 
 // pk: packed FP32 products (eighth form; FP32 with cp.async staging only)
+// pk 1: packed FP32 products (form 8); 2: the same with the signs in the
+// shared broadcast pairs (form 10)
 template <class T, int G>
 static void launch_contract4(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
                              const typename V2<T>::t* lines, int msl, int unroll_msl, bool bulk,
-                             bool pk, int mwlt, int R, double* partial,
+                             int pk, int mwlt, int R, double* partial,
                              const typename V2<T>::t* level, typename V2<T>::t* next,
                              cudaStream_t st) {
   if constexpr (sizeof(T) == 4) {
-    if (pk) {
-      launch_contract4_b<T, G, false, true>(g, p, u0, lines, msl, unroll_msl, mwlt, R, partial, level, next, st);
+    if (pk == 1) {
+      launch_contract4_b<T, G, false, 1>(g, p, u0, lines, msl, unroll_msl, mwlt, R, partial, level, next, st);
+      return;
+    }
+    if (pk == 2) {
+      launch_contract4_b<T, G, false, 2>(g, p, u0, lines, msl, unroll_msl, mwlt, R, partial, level, next, st);
       return;
     }
   }
@@ -1096,7 +1102,7 @@ static void launch_contract4(const Geo& g, const ContractPlan& p, const typename
     launch_contract4_b<T, G, false>(g, p, u0, lines, msl, unroll_msl, mwlt, R, partial, level, next, st);
 }
 
-template <class T, int G, int MSL, bool BULK, bool PK = false>
+template <class T, int G, int MSL, bool BULK, int PK = 0>
 static void launch_contract4_batch_m(const CArgs<T>* A, const long long* pre, int n,
                                      long long nblocks, int block, size_t smem, cudaStream_t st) {
   constexpr int MINB = (sizeof(T) == 4) ? ((G <= 3) ? 3 : 2) : ((G <= 1) ? 3 : 2);
@@ -1159,14 +1165,14 @@ void contract(const Geo& g, const ContractPlan& p, const typename V2<T>::t* u0,
     }
     return;
   }
-  if (p.variant >= 4 && p.variant <= 8) {
+  if ((p.variant >= 4 && p.variant <= 8) || p.variant == 10) {
     // form 5: form 4 with the level loops unrolled for msl 4-6; forms 6 / 7:
     // forms 5 / 4 with the top lines staged by bulk copies, where a time
     // slice is whole 32-site tiles (else they run as forms 5 / 4); form 8:
     // form 5 with packed FP32 products (the FP64 form runs form 5)
-    const int m = (p.variant == 5 || p.variant == 6 || p.variant == 8) ? msl : 0;
+    const int m = (p.variant == 5 || p.variant == 6 || p.variant == 8 || p.variant == 10) ? msl : 0;
     const bool bulk = (p.variant == 6 || p.variant == 7) && contract_can_bulk(g);
-    const bool pk = p.variant == 8;
+    const int pk = p.variant == 8 ? 1 : (p.variant == 10 ? 2 : 0);
     switch (p.G) {
       case 1: launch_contract4<T, 1>(g, p, u0, lines, msl, m, bulk, pk, mwlt, R, partial, level, next, st); return;
       case 2: launch_contract4<T, 2>(g, p, u0, lines, msl, m, bulk, pk, mwlt, R, partial, level, next, st); return;
