@@ -28,9 +28,10 @@ host threads, on full-size pieces of the workload; c1_measured_pair: the 8^4
 workload measured whole by the GPU and by the reference itself.
 
 --impl reference times the reference's own CPU implementation: its modules
-compiled from source (oracle/_ref, one process: without MPI the reference
-runs on one core), each step one full-size APE sweep, with HYP and the loop
-stage timed at full size in two further processes meanwhile.
+compiled from source (oracle/_ref), as one-core replicas on all host cores
+(without MPI the reference runs one process per core), each step one
+full-size APE sweep in every replica, with HYP and the loop stage timed at
+full size in two further replicas meanwhile.
 """
 from __future__ import annotations
 
@@ -110,17 +111,15 @@ def _loop_piece(p, mwlt):
     return _Parms(p.msl, [0] * p.msl, mwlt, 1)
 
 
-def _piece_worker(mwlt, n, bc, seed, eps, p, q):
+def _piece_worker(mwlt, path, n, bc, p, q):
     """Full-size pieces of the reference in their own process: hyp_links once,
     then the loop stage for r = 1, t = 1..mwlt on the HYP-smeared field.
     Puts {name: seconds}."""
     sys.path.insert(0, ROOT)
-    from tests import oracle as O
-    O.set_threads(1)
-    u = O.generate_links(n, bc, seed, eps)
+    import numpy as np
     from tests import refimpl as R
     ref = R.Ref(n)
-    ref.set_field(bc, u)
+    ref.set_field(bc, np.load(path, mmap_mode="r"))
     out = {}
     t0 = time.perf_counter()
     ref.hyp_links(*p.alpha_action, p.proj, p.proj_iter)
@@ -129,6 +128,35 @@ def _piece_worker(mwlt, n, bc, seed, eps, p, q):
     ref.wloop_sum(_loop_piece(p, mwlt))
     out[f"loops_t{mwlt}"] = time.perf_counter() - t0
     q.put(out)
+
+
+def _ape_worker(path, n, bc, p, nsteps, barrier, q):
+    """One replica of the reference: nsteps spatial APE sweeps of the full
+    field, each started together with the other replicas' (barrier).  Puts
+    the list of sweep times."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    from tests import refimpl as R
+    ref = R.Ref(n)
+    ref.set_field(bc, np.load(path, mmap_mode="r"))
+    ts = []
+    for _ in range(nsteps):
+        barrier.wait()
+        t0 = time.perf_counter()
+        ref.ape_links(p.alpha_ape, p.proj, p.proj_iter, time=0, nsweeps=1)
+        ts.append(time.perf_counter() - t0)
+    q.put(ts)
+
+
+def _mem_available_gb():
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable:"):
+                    return int(ln.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 0.0
 
 
 def _reference_c1(reps):
@@ -149,18 +177,25 @@ def _reference_c1(reps):
 
 def run_reference(args, rank):
     """The reference's own CPU implementation (oracle/_ref: its modules built
-    from source; one process, as without MPI) on the 32^3x64 workload.  Every
-    piece runs at the full size: each step is one spatial APE sweep of the
-    32^3x64 field (the ms10 run does 50); HYP and the loop stage for
-    (r=1, t=1) and for (r=1, t=1,2) run once each, in two further processes
-    (one core each) while the steps run.  The configs/s is then an estimate from measured pieces:
-    t_config = t_hyp + 50 t_ape + (t_fixed + 384 t_pair), with t_pair =
-    t(t<=2) - t(t<=1) and t_fixed = t(t<=1) - t_pair (the reference's loop
+    from source) on the 32^3x64 workload, on the host's cores.  Without MPI
+    the reference runs one process per core, so the host runs it as
+    independent replicas, one configuration stream each.  Every piece runs at
+    the full size and under the load of all the replicas: each step is one
+    spatial APE sweep (the ms10 run does 50 per configuration) in every APE
+    replica at once; two further replicas run HYP and the loop stage for
+    (r=1, t=1) and for (r=1, t=1,2) meanwhile.  Per replica a configuration
+    takes t_config = t_hyp + 50 t_ape + (t_fixed + 384 t_pair), with t_pair =
+    t(t<=2) - t(t<=1) and t_fixed = max(0, t(t<=1) - t_pair) (the reference's loop
     stage costs the same for every (r,t) pair at fixed msl, wloop.c:545-571;
-    r <= 16, t <= 24 is 384 pairs)."""
+    r <= 16, t <= 24 is 384 pairs), and the host's configs/s is the number of
+    replicas over t_config.  The replica count is the core count, lowered if
+    the host memory would not hold them (about 5 GB per APE replica, 22 GB
+    per loop replica)."""
     if rank != 0:
         return
     import multiprocessing as mp
+    import tempfile
+    import numpy as np
     from tests import oracle as O
     from tests import refimpl as R
     p = C3_P
@@ -168,62 +203,73 @@ def run_reference(args, rank):
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref was not built for 64x32x32x32 (make -C oracle ref)"}))
         return
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    procs = [ctx.Process(target=_piece_worker, args=(k, C3_N, C3_BC, C3_SEED, C3_EPS, p, q))
-             for k in (1, 2)]
+    cores = os.cpu_count() or 1
+    mem = _mem_available_gb()
+    n_ape = max(1, min(cores - 2, int((mem - 2 * 22 - 6) // 5)))
     wall0 = time.perf_counter()
+    O.set_threads(cores)
+    tmpdir = tempfile.mkdtemp(prefix="wlref_")
+    path = os.path.join(tmpdir, "c3_field.npy")
+    np.save(path, O.generate_links(C3_N, C3_BC, C3_SEED, C3_EPS))
+    ctx = mp.get_context("spawn")
+    q_piece, q_ape = ctx.Queue(), ctx.Queue()
+    nsteps = args.warmup + args.steps
+    barrier = ctx.Barrier(n_ape)
+    procs = [ctx.Process(target=_piece_worker, args=(k, path, C3_N, C3_BC, p, q_piece))
+             for k in (1, 2)]
+    procs += [ctx.Process(target=_ape_worker, args=(path, C3_N, C3_BC, p, nsteps, barrier, q_ape))
+              for _ in range(n_ape)]
     for pr in procs:
         pr.start()
-    O.set_threads(os.cpu_count() or 1)
-    u = O.generate_links(C3_N, C3_BC, C3_SEED, C3_EPS)
-    ref = R.Ref(C3_N)
-    ref.set_field(C3_BC, u)
-    steps = []
-    for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        ref.ape_links(p.alpha_ape, p.proj, p.proj_iter, time=0, nsweeps=1)
-        dt = time.perf_counter() - t0
-        if i >= args.warmup:
-            steps.append(dt)
+    ape = [q_ape.get() for _ in range(n_ape)]
     pieces = {}
-    for _ in procs:
-        pieces.update(q.get())
+    for _ in range(2):
+        pieces.update(q_piece.get())
     for pr in procs:
         pr.join()
+    os.remove(path)
+    os.rmdir(tmpdir)
+    # a step ends when the slowest replica's sweep ends
+    steps = [max(ts[i] for ts in ape) for i in range(args.warmup, nsteps)]
+    t_ape = statistics.mean(steps)
     pieces["hyp"] = 0.5 * (pieces["hyp_1"] + pieces["hyp_2"])
     t_c1 = _reference_c1(3)
-    t_ape = statistics.mean(steps)
     sweeps = sum(p.nss[:p.msl])
     pairs = p.mwlr * p.mwlt
     t_pair = pieces["loops_t2"] - pieces["loops_t1"]
-    t_fixed = pieces["loops_t1"] - t_pair
+    # the one-time part of the loop stage, never below zero (the two loop
+    # pieces run in different replicas and their load can differ a little)
+    t_fixed = max(0.0, pieces["loops_t1"] - t_pair)
     t_cfg = pieces["hyp"] + sweeps * t_ape + t_fixed + pairs * t_pair
-    value = 1.0 / t_cfg
-    sample = (f"the reference's modules built from source (oracle/_ref), one process per piece "
-              f"(one core each), at the full 32^3x64 size: hyp_links {pieces['hyp']:.1f} s "
-              f"(mean of 2); one spatial APE sweep "
-              f"{t_ape:.2f} s (mean of {len(steps)} timed steps; 50 per configuration); loop "
-              f"stage r=1,t=1 {pieces['loops_t1']:.1f} s and r=1,t<=2 {pieces['loops_t2']:.1f} s "
-              f"(per (r,t) pair {t_pair:.1f} s, 384 pairs); configs/s estimated from these "
-              f"measured pieces")
+    replicas = n_ape + 2
+    value = replicas / t_cfg
+    sample = (f"the reference's modules built from source (oracle/_ref), {replicas} one-core "
+              f"replicas at once on {cores} cores, at the full 32^3x64 size: one spatial APE "
+              f"sweep {t_ape:.2f} s ({n_ape} replicas in step, mean of {len(steps)} timed "
+              f"steps; 50 per configuration); hyp_links {pieces['hyp']:.1f} s; loop stage "
+              f"r=1,t=1 {pieces['loops_t1']:.1f} s and r=1,t<=2 {pieces['loops_t2']:.1f} s (per "
+              f"(r,t) pair {t_pair:.1f} s, 384 pairs); {t_cfg:.0f} s per configuration and "
+              f"replica, configs/s = replicas / that")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ape * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": C3_DESC, "parallelism": "one process (the reference "
-                       "without MPI runs on one core)"},
-            "step": "one full-size spatial APE sweep of the reference (ape_spatial_links)",
-            "value_kind": "estimate from full-size measured pieces",
+            "config": {"workload": C3_DESC, "parallelism": f"{replicas} replicas of the "
+                       f"one-process reference (no MPI), one per core"},
+            "step": f"one full-size spatial APE sweep (ape_spatial_links) in each of {n_ape} "
+                    f"replicas at once",
+            "value_kind": "estimate from full-size pieces measured under the load of all replicas",
             "pieces_s": {"hyp": pieces["hyp"], "hyp_runs": [pieces["hyp_1"], pieces["hyp_2"]],
                          "ape_sweep": t_ape,
                          "loops_r1_t1": pieces["loops_t1"], "loops_r1_t2": pieces["loops_t2"],
-                         "per_pair": t_pair, "fixed": t_fixed, "config_estimate": t_cfg},
+                         "per_pair": t_pair, "fixed": t_fixed, "config_per_replica": t_cfg},
+            "replicas": replicas, "host_memory_available_gb": mem,
             "wall_s": time.perf_counter() - wall0,
             "c1_measured": {"workload": "c1: 8^4 periodic, eps 0.3, HYP2, APE 0.5 nss 0 5 5 5, "
                                         "msl 4, r,t<=4", "seconds_per_config": t_c1,
-                            "configs_per_s": 1.0 / t_c1, "kind": "reference, whole measurement"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                            "configs_per_s_one_core": 1.0 / t_c1,
+                            "kind": "reference, whole measurement, one core"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": replicas, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -250,7 +296,7 @@ def cpu_sample(threads: int):
     t4 = time.perf_counter()
     sweeps = sum(p.nss[:p.msl])
     t_pair = (t4 - t3) - (t3 - t2)
-    t_fixed = (t3 - t2) - t_pair
+    t_fixed = max(0.0, (t3 - t2) - t_pair)
     t_cfg = (t1 - t0) + sweeps * (t2 - t1) + t_fixed + p.mwlr * p.mwlt * t_pair
     sample = (f"oracle on {threads} threads at the full 32^3x64 size: HYP {t1 - t0:.2f} s, one "
               f"APE sweep {t2 - t1:.3f} s (x{sweeps}), loop stage r=1,t=1 {t3 - t2:.2f} s and "
