@@ -167,7 +167,8 @@ def test_tune_context_picks_a_shape_with_the_same_result(tmp_path, monkeypatch):
     with Context(n, bc, "mixed") as c:
         c.generate(5, 0.3)
         c.snapshot()
-        base = c.measure(p)
+        base = c.measure(p)  # HYP-smears the field in place
+        c.restore()  # the tuner snapshots the field it is given
         shape = autotune.tune_context(c, p, "mixed", use_cache=False)
         c.restore()
         got = c.measure(p)

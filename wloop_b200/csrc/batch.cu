@@ -465,13 +465,13 @@ int plan(wlg_batch* b) {
     // FP64 kernel spills), SB = 4 the fourth with bulk-copy staging (the FP64
     // default where a time slice is whole 32-site tiles; lattices that are not
     // run the fourth form), SB 5 the unrolled fourth form with packed FP32
-    // products (the eighth form; the FP32 default, as for a single lattice;
-    // an FP64 batch runs SB 3)
+    // products, their signs in the shared broadcast pairs (the tenth form;
+    // the FP32 default, as for a single lattice; an FP64 batch runs SB 3)
     f.cp.SB = b->tG ? b->tSB : (fp64 ? 4 : 5);
     if (f.cp.SB == 4 && !contract_can_bulk(f.g)) f.cp.SB = 0;
     if (f.cp.SB == 5 && fp64) f.cp.SB = 3;
     f.cp.variant = (f.cp.SB == 1 || f.cp.SB == 2) ? 3
-                 : (f.cp.SB == 3 ? 5 : (f.cp.SB == 4 ? 7 : (f.cp.SB == 5 ? 8 : 4)));
+                 : (f.cp.SB == 3 ? 5 : (f.cp.SB == 4 ? 7 : (f.cp.SB == 5 ? 10 : 4)));
     if (f.cp.G > 4) {
       set_error("batch: contraction shape G=%d is not available in batched form", f.cp.G);
       return -1;

@@ -240,10 +240,12 @@ ContractPlan contract_plan(const Geo& g, int msl, int mwlt, bool fp64, int G_hin
   // fourth form (staged top lines, shared-memory reduction) unless G = 6,
   // which only the second form has: in FP32 with its level loops unrolled,
   // packed two-lane FMA products and the next level's line read ahead (form
-  // 8; 4.6 % faster than form 5 at 32^3x64), in FP64 with the top lines staged by
+  // 8; 4.6 % faster than form 5 at 32^3x64) with the products' signs in the
+  // shared broadcast pairs (form 10; the same result, 1.9 % faster than form
+  // 8), in FP64 with the top lines staged by
   // bulk copies (form 7; 5 % faster there, 2 % slower in FP32; the unrolled
   // FP64 kernel spills registers)
-  p.variant = (G <= 4) ? (fp64 ? 7 : 8) : 2;
+  p.variant = (G <= 4) ? (fp64 ? 7 : 10) : 2;
   p.ngrp = (msl + G - 1) / G;
   // FP64 stages twice the bytes per thread: 64-thread blocks keep 3 blocks per SM
   p.block = block_hint > 0 ? block_hint : ((fp64 && p.variant >= 4) ? 64 : 128);
@@ -1117,7 +1119,8 @@ static void launch_contract4_batch_m(const CArgs<T>* A, const long long* pre, in
 }
 
 // msl: the level count shared by every lattice of the launch, or 0
-// pk: packed FP32 products (eighth form, cp.async staging; FP32 only)
+// pk: packed FP32 products with the signs in the shared broadcast pairs (tenth
+// form, cp.async staging; FP32 only)
 template <class T, int G>
 static void launch_contract4_batch(const CArgs<T>* A, const long long* pre, int n, long long nblocks,
                                    int block, size_t smem, int msl, bool bulk, bool pk,
@@ -1125,10 +1128,10 @@ static void launch_contract4_batch(const CArgs<T>* A, const long long* pre, int 
   if constexpr (sizeof(T) == 4) {
     if (pk && !bulk) {
       switch (msl_variant(msl)) {
-        case 4: launch_contract4_batch_m<T, G, 4, false, true>(A, pre, n, nblocks, block, smem, st); return;
-        case 5: launch_contract4_batch_m<T, G, 5, false, true>(A, pre, n, nblocks, block, smem, st); return;
-        case 6: launch_contract4_batch_m<T, G, 6, false, true>(A, pre, n, nblocks, block, smem, st); return;
-        default: launch_contract4_batch_m<T, G, 0, false, true>(A, pre, n, nblocks, block, smem, st); return;
+        case 4: launch_contract4_batch_m<T, G, 4, false, 2>(A, pre, n, nblocks, block, smem, st); return;
+        case 5: launch_contract4_batch_m<T, G, 5, false, 2>(A, pre, n, nblocks, block, smem, st); return;
+        case 6: launch_contract4_batch_m<T, G, 6, false, 2>(A, pre, n, nblocks, block, smem, st); return;
+        default: launch_contract4_batch_m<T, G, 0, false, 2>(A, pre, n, nblocks, block, smem, st); return;
       }
     }
   }
