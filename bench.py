@@ -141,7 +141,7 @@ def _ape_worker(path, n, bc, p, nsteps, barrier, q):
     ref.set_field(bc, np.load(path, mmap_mode="r"))
     ts = []
     for _ in range(nsteps):
-        barrier.wait()
+        barrier.wait(timeout=600)  # a replica that died breaks the barrier
         t0 = time.perf_counter()
         ref.ape_links(p.alpha_ape, p.proj, p.proj_iter, time=0, nsweeps=1)
         ts.append(time.perf_counter() - t0)
@@ -221,14 +221,25 @@ def run_reference(args, rank):
               for _ in range(n_ape)]
     for pr in procs:
         pr.start()
-    ape = [q_ape.get() for _ in range(n_ape)]
-    pieces = {}
-    for _ in range(2):
-        pieces.update(q_piece.get())
+    import queue
+    try:
+        # every piece is minutes of work; an hour means a replica died
+        ape = [q_ape.get(timeout=3600) for _ in range(n_ape)]
+        pieces = {}
+        for _ in range(2):
+            pieces.update(q_piece.get(timeout=3600))
+    except queue.Empty:
+        for pr in procs:
+            if pr.is_alive():
+                pr.terminate()
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "a replica of the reference did not report (died or ran out of memory)"}))
+        return
+    finally:
+        os.remove(path)
+        os.rmdir(tmpdir)
     for pr in procs:
         pr.join()
-    os.remove(path)
-    os.rmdir(tmpdir)
     # a step ends when the slowest replica's sweep ends
     steps = [max(ts[i] for ts in ape) for i in range(args.warmup, nsteps)]
     t_ape = statistics.mean(steps)
