@@ -129,6 +129,71 @@ def test_run_single_process_with_fake_measure(tmp_path):
 
 
 # ---------------------------------------------------------------------------
+# ms10's file safety, continuation (-a), end flag and backups
+# ---------------------------------------------------------------------------
+def _fake(head):
+    return lambda nc: fake_wl(nc, head[0])
+
+
+def test_new_run_refuses_to_overwrite(tmp_path):
+    head = M.dat_head(P, N[0])
+    M.run(M.Run("o", N, 3, P, first=1, last=3), str(tmp_path), measure=_fake(head))
+    with pytest.raises(WlgError, match="overwrite"):
+        M.run(M.Run("o", N, 3, P, first=1, last=3), str(tmp_path), measure=_fake(head))
+
+
+def test_continuation_run_equals_one_run(tmp_path):
+    head = M.dat_head(P, N[0])
+    M.run(M.Run("c", N, 3, P, first=1, last=5, step=2), str(tmp_path / "a"), measure=_fake(head))
+    res = M.run(M.Run("c", N, 3, P, first=7, last=11, step=2), str(tmp_path / "a"),
+                measure=_fake(head), continue_run=True)
+    assert res["configs"] == [7, 9, 11]
+    M.run(M.Run("c", N, 3, P, first=1, last=11, step=2), str(tmp_path / "b"), measure=_fake(head))
+    a = open(M.dat_path(str(tmp_path / "a"), "c"), "rb").read()
+    b = open(M.dat_path(str(tmp_path / "b"), "c"), "rb").read()
+    assert a == b
+    log = open(M.log_path(str(tmp_path / "a"), "c")).read()
+    assert log.count("fully processed") == 6
+    # the backups follow the files
+    for f in (M.dat_path(str(tmp_path / "a"), "c"), M.log_path(str(tmp_path / "a"), "c")):
+        assert open(f, "rb").read() == open(f + "~", "rb").read()
+
+
+@pytest.mark.parametrize("first,step,parms,match", [
+    (9, 2, P, "does not continue"),
+    (7, 3, P, "different configuration separation"),
+    (7, 2, WloopParms(msl=3, nss=[0, 1, 3], mwlt=3, mwlr=2, op_smear=APE, alpha_ape=0.5,
+                      proj_iter=4), "do not match"),
+])
+def test_continuation_checks(tmp_path, first, step, parms, match):
+    head = M.dat_head(P, N[0])
+    M.run(M.Run("k", N, 3, P, first=1, last=5, step=2), str(tmp_path), measure=_fake(head))
+    with pytest.raises(WlgError, match=match):
+        M.run(M.Run("k", N, 3, parms, first=first, last=first + 4, step=step), str(tmp_path),
+              measure=_fake(head), continue_run=True)
+
+
+def test_continuation_refuses_an_inconsistent_log(tmp_path):
+    head = M.dat_head(P, N[0])
+    M.run(M.Run("g", N, 3, P, first=1, last=5, step=2), str(tmp_path), measure=_fake(head))
+    with open(M.log_path(str(tmp_path), "g"), "a") as f:
+        f.write("Configuration no 7 fully processed in 1.00e+00 sec\n")
+    with pytest.raises(WlgError, match="not as reported in the log"):
+        M.run(M.Run("g", N, 3, P, first=9, last=9), str(tmp_path), measure=_fake(head),
+              continue_run=True)
+
+
+def test_end_flag_stops_the_run(tmp_path):
+    head = M.dat_head(P, N[0])
+    open(M.end_path(str(tmp_path), "e"), "w").close()
+    res = M.run(M.Run("e", N, 3, P, first=1, last=9), str(tmp_path), measure=_fake(head))
+    assert res["configs"] == [1]
+    assert not os.path.exists(M.end_path(str(tmp_path), "e"))
+    assert M.count(M.dat_path(str(tmp_path), "e"))[1] == 1
+    assert "End flag set, run stopped" in open(M.log_path(str(tmp_path), "e")).read()
+
+
+# ---------------------------------------------------------------------------
 # two replicas over gloo
 # ---------------------------------------------------------------------------
 def _free_port() -> int:

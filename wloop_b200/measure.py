@@ -220,6 +220,52 @@ def log_path(out_dir: str, name: str) -> str:
     return os.path.join(out_dir, f"{name}.ms10.log")
 
 
+def end_path(out_dir: str, name: str) -> str:
+    """ms10's end flag (ms10.c:662-680): a file of this name stops the run
+    after the configuration in progress."""
+    return os.path.join(out_dir, f"{name}.ms10.end")
+
+
+def _equally_spaced(ncs: Sequence[int], what: str) -> Tuple[int, int, int]:
+    """(first, last, step) of a list of configuration numbers; they must be
+    equally spaced (check_old_log / check_old_dat, ms10.c:374-487)."""
+    if not ncs:
+        raise WlgError(f"{what}: No data records found")
+    step = ncs[1] - ncs[0] if len(ncs) > 1 else 0
+    if any(b - a != step for a, b in zip(ncs, ncs[1:])):
+        raise WlgError(f"{what}: Configuration numbers are not equally spaced")
+    return ncs[0], ncs[-1], step
+
+
+def check_continuation(r: Run, out_dir: str) -> int:
+    """ms10's continuation checks (-a, ms10.c:490-526): the old log and .dat
+    report the same equally spaced configurations, the .dat head and the .par
+    records (bc, then wloop) are this run's, and the run continues the old
+    range at last + step.  Returns the number of records already there."""
+    logf, dat, par = log_path(out_dir, r.name), dat_path(out_dir, r.name), par_path(out_dir, r.name)
+    for p in (logf, dat, par):
+        if not os.path.exists(p):
+            raise WlgError(f"check_files: continuation run: {p} does not exist")
+    done = []
+    with open(logf) as f:
+        for ln in f:
+            if ln.startswith("Configuration no ") and "fully processed" in ln:
+                done.append(int(ln.split()[2]))
+    fst, lst, stp = _equally_spaced(done, "check_old_log")
+    check_head(dat, dat_head(r.parms, r.n[0]))
+    _, ncs, _ = read(dat)
+    if (fst, lst, stp) != _equally_spaced([int(x) for x in ncs], "check_old_dat"):
+        raise WlgError("check_old_dat: Configuration range is not as reported in the log file")
+    check_par(par, r.parms, bc=r.bc)
+    if fst != lst and stp != r.step:
+        raise WlgError("check_files: Continuation run: "
+                       "Previous run had a different configuration separation")
+    if r.first != lst + r.step:
+        raise WlgError("check_files: Continuation run: "
+                       "Configuration range does not continue the previous one")
+    return len(ncs)
+
+
 def _device_measure(run: Run, source, device: int, cnfg_dir: Optional[str] = None):
     """nc -> (wl_mat, average plaquette after HYP, average plaquette of every
     level): hyp_links(alpha_action) then wloop_sum, as Context.measure."""
@@ -245,7 +291,8 @@ def _device_measure(run: Run, source, device: int, cnfg_dir: Optional[str] = Non
 def run(r: Run, out_dir: str, replicas: Optional[Replicas] = None,
         source: Optional[Callable[[int], np.ndarray]] = None,
         measure: Optional[Callable[[int], np.ndarray]] = None,
-        log: Optional[Callable[[str], None]] = None, cnfg_dir: Optional[str] = None) -> dict:
+        log: Optional[Callable[[str], None]] = None, cnfg_dir: Optional[str] = None,
+        continue_run: bool = False, backup: bool = True) -> dict:
     """Measures this rank's share of the run's configurations and appends one
     record per configuration to its .dat file.  `measure` (nc -> wl_mat)
     replaces the device measurement; by default a Context on this rank's
@@ -254,22 +301,38 @@ def run(r: Run, out_dir: str, replicas: Optional[Replicas] = None,
     Every rank writes its lines to <name>.ms10.log (rank r > 0 to
     <name>.ms10.r<rank>.log) and to `log`.  With several replicas, rank 0
     merges the per-rank files into <name>.ms10.dat after all ranks have
-    finished."""
+    finished.
+
+    As ms10 (ms10.c:490-526, 662-680, 737-738): a new run refuses to
+    overwrite an old <name>.ms10.log or .ms10.dat; continue_run=True continues an
+    old run of one process (check_continuation) and adds its records and log
+    lines to the old files; a file <name>.ms10.end stops a one-process run
+    after the configuration in progress (the file is removed); with backup
+    the log and .dat are copied to <file>~ after every configuration."""
+    import shutil
     rank = replicas.rank if replicas else 0
     world = replicas.world if replicas else 1
     local = replicas.device if replicas else 0
     os.makedirs(out_dir, exist_ok=True)
     head = dat_head(r.parms, r.n[0])
     path = dat_path(out_dir, r.name, rank, world)
-    write_head(path, head)
-    if rank == 0:
-        par = par_path(out_dir, r.name)
-        if os.path.exists(par):
-            os.remove(par)
-        write_par(par, r.parms, r.bc)
+    if continue_run:
+        if world > 1:
+            raise WlgError("check_files: a continuation run has one process")
+        check_continuation(r, out_dir)
+    else:
+        if rank == 0 and any(os.path.exists(p) for p in (log_path(out_dir, r.name),
+                                                         dat_path(out_dir, r.name))):
+            raise WlgError("check_files: Attempt to overwrite old *.log or *.dat file")
+        write_head(path, head)
+        if rank == 0:
+            par = par_path(out_dir, r.name)
+            if os.path.exists(par):
+                os.remove(par)
+            write_par(par, r.parms, r.bc)
     logfile = log_path(out_dir, r.name) if rank == 0 else \
         os.path.join(out_dir, f"{r.name}.ms10.r{rank}.log")
-    flog = open(logfile, "w")
+    flog = open(logfile, "a" if continue_run else "w")
 
     def say(line: str) -> None:
         flog.write(line + "\n")
@@ -281,7 +344,7 @@ def run(r: Run, out_dir: str, replicas: Optional[Replicas] = None,
     ctx = None
     if measure is None:
         ctx, measure = _device_measure(r, source, local, cnfg_dir)
-    seconds = []
+    seconds, processed = [], []
     cum = np.cumsum(r.parms.nss[:r.parms.msl])
     try:
         for nc in mine:
@@ -293,6 +356,7 @@ def run(r: Run, out_dir: str, replicas: Optional[Replicas] = None,
                 raise WlgError(f"measurement of configuration {nc} has {wl.size} entries, "
                                f"expected {head[0]}")
             append(path, nc, wl)
+            processed.append(nc)
             seconds.append(time.perf_counter() - t0)
             if isinstance(res, tuple):
                 say(f"Average plaquette after HYP smearing = {res[1]:.15e}")
@@ -301,11 +365,19 @@ def run(r: Run, out_dir: str, replicas: Optional[Replicas] = None,
                         f"{v:.15e}")
             say(f"Configuration no {nc} fully processed in {seconds[-1]:.2e} sec "
                 f"(average = {sum(seconds) / len(seconds):.2e} sec)")
+            if backup:
+                shutil.copyfile(logfile, logfile + "~")
+                shutil.copyfile(path, path + "~")
+            endf = end_path(out_dir, r.name)
+            if world == 1 and os.path.exists(endf):
+                os.remove(endf)
+                say("End flag set, run stopped")
+                break
     finally:
         flog.close()
         if ctx is not None:
             ctx.close()
-    out = {"rank": rank, "world": world, "path": path, "configs": mine, "seconds": seconds,
+    out = {"rank": rank, "world": world, "path": path, "configs": processed, "seconds": seconds,
            "log": logfile}
     if world > 1:
         replicas.barrier()
@@ -350,6 +422,8 @@ def main(argv=None) -> int:
     ap.add_argument("--alpha-action", type=float, nargs=3, default=(1.0, 1.0, 0.5))
     ap.add_argument("--alpha", type=float, nargs="+", default=[0.5])
     ap.add_argument("--proj-iter", type=int, default=4)
+    ap.add_argument("-a", "--append", action="store_true",
+                    help="continue an old run (ms10 -a): check its files and append")
     a = ap.parse_args(argv)
     n = tuple(int(x) for x in a.lattice.split("x"))
     hyp = a.op_smear == "HYP"
@@ -358,7 +432,8 @@ def main(argv=None) -> int:
                    a.proj_iter)
     r = Run(a.name, n, a.bc, p, a.first, a.last, a.step, a.precision, a.eps)
     with Replicas() as rep:
-        res = run(r, a.out, rep, log=print if rep.rank == 0 else None, cnfg_dir=a.cnfg_dir)
+        res = run(r, a.out, rep, log=print if rep.rank == 0 else None, cnfg_dir=a.cnfg_dir,
+                  continue_run=a.append)
     if res.get("merged"):
         print(f"{res['records']} records in {res['merged']}")
     return 0
