@@ -371,6 +371,14 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def gram_flops_per_launch(w):
+    """Flops of one banded Gram launch: every (x0, T, s1, s2) is a dot product
+    over 3 directions x vs sites x 18 components."""
+    p = w.parms
+    vs = w.volume // w.n[0]
+    return 2.0 * w.n[0] * p.mwlt * p.msl * p.msl * 3 * vs * 18
+
+
 def load_traffic():
     p = os.path.join(ROOT, "profiles", "contract_traffic.json")
     if os.path.exists(p):
@@ -430,7 +438,8 @@ def run_ours(args, rank, world, local):
         ck = clocks.stop()
         barrier()
         ms = e0.elapsed_time(e1) / steps
-        kt = {k: ctx.kernel_time(k) for k in ("hyp", "ape", "plaq", "lines", "contract", "reduce")}
+        kt = {k: ctx.kernel_time(k)
+              for k in ("hyp", "ape", "plaq", "gauge", "lines", "contract", "reduce")}
         ctx.set_profiling(False)
         return ctx, ms, wl, kt, ck, l1 - l0
 
@@ -439,6 +448,7 @@ def run_ours(args, rank, world, local):
                                                          True)
     ms_max = barrier_max(ms)
     value = world * 1000.0 / ms_max
+    form = ctx.contract_form
 
     # ---- e2e through the public API from pinned host memory ----
     e2e = None
@@ -504,8 +514,12 @@ def run_ours(args, rank, world, local):
     # ---- roofline of the dominant kernel (contraction) ----
     c_ms, c_n = kt["contract"]
     per_launch_ms = c_ms / max(1, c_n)
-    # the contraction launches also carry the spatial line step of the next R
-    flops_per_launch = (fl["contract"] + fl["lines"]) / p.mwlr
+    if form == 11:
+        # the banded Gram product: 2 N0 mwlt msl^2 (3 vs 18) flops per R
+        flops_per_launch = gram_flops_per_launch(w)
+    else:
+        # the contraction launches also carry the spatial line step of the next R
+        flops_per_launch = (fl["contract"] + fl["lines"]) / p.mwlr
     achieved = flops_per_launch / (per_launch_ms * 1e-3) / 1e12
     peak = peak_tflops(args.precision, local)
     peak_src = "vector FMA probe measured in this run (wlg_peak_flops, fma.rn.f64; of measured)"
@@ -518,7 +532,7 @@ def run_ours(args, rank, world, local):
         peak = max(p_scalar, p_x2)
         peak_src = ("vector FMA probe measured in this run (wlg_peak_flops): the higher of "
                     "scalar fma.rn.f32 and packed fma.rn.f32x2 chains; of measured")
-    traffic = load_traffic().get(args.precision)
+    traffic = load_traffic().get(args.precision + ("_gram" if form == 11 else ""))
     peaks_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
     hbm, hbm_src = None, None
     if os.path.exists(peaks_file):
@@ -534,14 +548,22 @@ def run_ours(args, rank, world, local):
     # lines out (2 x 3 msl V, for 15 of the 16 launches)
     link_b = 72 if args.precision == "mixed" else 144
     vol = w.volume
-    bytes_per_launch = link_b * vol * ((3 * p.msl + 1) + 6 * p.msl * (p.mwlr - 1) / p.mwlr)
+    if form == 11:
+        # its A lines (N0 slices) and B lines (N0 + mwlt slices, periodic), once
+        nu = w.n[0] + (p.mwlt if w.bc != 0 else 0)
+        bytes_per_launch = link_b * (w.n[0] + nu) * (vol // w.n[0]) * 3 * p.msl
+        kname = "k_gram (banded Gram product of the temporal-gauge lines)"
+    else:
+        bytes_per_launch = link_b * vol * ((3 * p.msl + 1) + 6 * p.msl * (p.mwlr - 1) / p.mwlr)
+        kname = "k_contract4 (loop contraction with the fused spatial line step)"
     hbm_ach = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
-    roof = {"kernel": "k_contract4 (loop contraction with the fused spatial line step)",
+    roof = {"kernel": kname, "contract_form": form,
             "bound": "fp32" if args.precision == "mixed" else "fp64",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": peak_src + "; the kernel is bound by CUDA-core FMA throughput, not "
-                           "by HBM or tensor cores (3x3 complex products have no tensor-core "
-                           "form), and MEASURED_PEAKS.json has no CUDA-core peak",
+                           "by HBM (its FP32 dot products need more precision than one "
+                           "TF32/BF16 tensor-core pass gives), and MEASURED_PEAKS.json has no "
+                           "CUDA-core peak",
             "peak_probes_tflops": peaks_probe,
             "flops_per_launch": flops_per_launch, "ms_per_launch": per_launch_ms,
             "traffic": traffic,

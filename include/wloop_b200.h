@@ -273,9 +273,22 @@ int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
  * 32-column chunk per warp, 72-byte line staging and per-warp partial
  * records, for four blocks per SM, FP32 contexts with msl 4-6 and the
  * default G only; 10: form 8 with the signs of the packed products in the
- * shared broadcast pairs, the same result) and SB top levels per reduction
- * (1 or 2; form 3 only). */
+ * shared broadcast pairs, the same result; 11: the temporal-gauge form, the
+ * default) and SB top levels per reduction (1 or 2; form 3 only).
+ *
+ * The temporal-gauge form (11) transforms the smeared links to the gauge in
+ * which the temporal lines are unit matrices (g(x0) = U0(0) ... U0(x0-1),
+ * exact for links that are unitary only approximately) and evaluates every
+ * loop as a dot product of two transformed lines: a banded Gram product.  It
+ * is used for every measurement unless another form is asked for here, and
+ * it falls back to the default carried-line form (7 FP64, 10 mixed) when
+ * g g^dag differs from 1 by more than 1/4 anywhere (links smeared without
+ * projection) or when msl and mwlt do not fit its kernel; wlg_contract_form
+ * tells which form ran.  After it the spatial lines that
+ * wlg_download_lines returns are rebuilt from the level store on request. */
 int wlg_set_contract_tuning(wlg_ctx* ctx, int variant, int G, int SB, int nCB, int block);
+/* The contraction form the last measurement on ctx used (0: none yet). */
+int wlg_contract_form(wlg_ctx* ctx, int* form);
 /* The context's CUDA stream (cudaStream_t), for callers that record events. */
 void* wlg_stream(wlg_ctx* ctx);
 /* Number of wloop_b200 kernel launches issued by this process so far. */

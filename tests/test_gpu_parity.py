@@ -15,6 +15,7 @@ import pytest
 
 from tests import lattice_np as L
 from tests import oracle as O
+from tests.forms import carried_form
 from wloop_b200 import APE, HYP, Context, WloopParms, approx_project_to_su3, generate_links
 from wloop_b200.api import staple_sum
 
@@ -340,6 +341,7 @@ def test_contract_shapes(case, prec):
     n, bc, p = CASES[case]
     u = generate_links(n, bc, 300 + case, 0.25)
     with Context(n, bc, prec) as c:
+        c.set_contract_tuning(variant=carried_form(prec))
         c.upload(u)
         c.snapshot()
         ref = c.measure(p)
@@ -412,13 +414,14 @@ def test_lines_left_by_the_measurement(prec, form):
 @pytest.mark.parametrize("case", [0, 3, 4])
 def test_ninth_form_matches_default(case):
     """The ninth contraction form (one 32-column chunk per warp, per-warp
-    partial records) gives the default form's mixed result up to the order of
+    partial records) gives the tenth form's mixed result up to the order of
     the FP64 sums, and the oracle's within 1e-6 plain relative."""
     n, bc, p = CASES[case]
     u = generate_links(n, bc, 700 + case, 0.25)
     uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
     ref = O.wloop_sum(n, bc, uh, p)
     with Context(n, bc, "mixed") as c:
+        c.set_contract_tuning(variant=10)
         c.upload(u)
         base = c.measure(p)
         c.set_contract_tuning(variant=9)

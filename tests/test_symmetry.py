@@ -172,3 +172,27 @@ def test_bounded_wait_ends():
         c.set_contract_tuning(7, 3, 0, 0, 64)
         w1 = c.measure(p)
     assert np.all(np.isfinite(w1))
+
+
+def test_largest_serving_volume_invariances():
+    """48^3x96 with open boundary conditions, the largest lattice of the
+    serving mix (HYP2 + 4 APE levels, msl 4, r,t <= 24), mixed form: gauge
+    invariance and a spatial translation by (0,1,-1,2), which leaves every
+    per-slice W unchanged."""
+    from wloop_b200.workloads import SERVE_VOLUMES, serving_request
+    n = SERVE_VOLUMES[-1]
+    w = next(serving_request(i) for i in range(1000) if serving_request(i).n == n)
+    p = w.parms
+    vol = int(np.prod(n))
+    with Context(n, 0, "mixed") as c:
+        c.generate(w.seed, w.eps)
+        c.snapshot()
+        w0 = c.measure(p)
+        c.restore()
+        c.gauge_transform(99, 1.0)
+        wg = c.measure(p)
+        c.restore()
+        c.shift_ud((0, 1, -1, 2))
+        ws = c.measure(p)
+    assert rel_dev(wg, w0) < max(tol_gauge(p, vol), 1e-6)
+    assert rel_dev(ws, w0) < max(tol_shift(p, vol), 1e-6)

@@ -91,6 +91,7 @@ def _load():
         "wlg_set_contract_shape": (i, [vp, i, i, i]),
         "wlg_set_contract_tuning": (i, [vp, i, i, i, i, i]),
         "wlg_stream": (vp, [vp]),
+        "wlg_contract_form": (i, [vp, ip]),
         "wlg_launch_count": (C.c_longlong, []),
         "wlg_snapshot": (i, [vp]),
         "wlg_gauge_transform": (i, [vp, u64, d]),

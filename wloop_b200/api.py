@@ -273,6 +273,13 @@ class Context:
               "set_contract_tuning")
 
     @property
+    def contract_form(self) -> int:
+        """Contraction form of the last measurement (11: temporal gauge; 0: none yet)."""
+        f = C.c_int(0)
+        check(lib.wlg_contract_form(self._h, C.byref(f)), "contract_form")
+        return f.value
+
+    @property
     def stream(self) -> int:
         """cudaStream_t of the context (for event timing by the caller)."""
         return lib.wlg_stream(self._h) or 0

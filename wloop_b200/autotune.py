@@ -1,7 +1,9 @@
 """Autotuner for the contraction kernel's shape (the dominant kernel).
 
 A shape is (G bottom levels per thread, SB top levels per reduction, threads
-per block, column blocks per (x0, level group)).  The tuner times every
+per block, column blocks per (x0, level group)); SB 9 and 11 mark the ninth
+and the temporal-gauge forms, and a context is timed over its whole loop
+stage (gauge transformation, line steps, contraction, reduction).  The tuner times every
 candidate on the caller's own data -- a Context (one lattice) or a Batch
 (many) -- through the C ABI, keeps the fastest, and caches it on disk keyed by
 precision, lattices and loop parameters, so later runs of the same workload
@@ -71,12 +73,24 @@ def candidates(msl: int, fp64: bool, batched: bool) -> List[Shape]:
         # the ninth form (one 32-column chunk per warp, four blocks per SM),
         # marked SB 9; single contexts only, with its own G and block
         out.append(((msl + 1) // 2, 9, 128, 0))
+    if not batched:
+        # the temporal-gauge form (banded Gram product), marked SB 11; it
+        # plans its own shapes
+        out.insert(0, (0, 11, 0, 0))
     return out
 
 
-def _apply(ctx, shape: Shape) -> None:
+def _apply(ctx, shape: Shape, fp64: bool) -> None:
     G, SB, block, nCB = shape
-    ctx.set_contract_tuning(_form(G, SB), G, SB if SB <= 2 else 0, nCB, block)
+    if SB == 11:
+        ctx.set_contract_tuning(11)
+        return
+    ctx.set_contract_tuning(_form(G, SB, fp64), G, SB if SB <= 2 else 0, nCB, block)
+
+
+# the timed scopes of one measurement's loop stage (the temporal-gauge form
+# runs its line steps and gauge transformation outside the contraction)
+LOOP_SCOPES = ("gauge", "lines", "contract", "reduce")
 
 
 def key_for(precision: str, lattices: Sequence[tuple], parms) -> str:
@@ -92,14 +106,15 @@ def cached(key: str) -> Optional[Shape]:
 def tune_context(ctx, parms, precision: str, reps: int = 1, use_cache: bool = True) -> Shape:
     """Times the contraction of a Context on its current field (the field is
     restored from a snapshot before every run) and applies the best shape."""
+    fp64 = precision == "fp64"
     key = key_for(precision, [ctx.n], parms)
     if use_cache and cached(key):
-        _apply(ctx, cached(key))
+        _apply(ctx, cached(key), fp64)
         return cached(key)
     ctx.snapshot()
     best, best_t = None, float("inf")
-    for (G, SB, block, nCB) in candidates(parms.msl, precision == "fp64", batched=False):
-        _apply(ctx, (G, SB, block, nCB))
+    for (G, SB, block, nCB) in candidates(parms.msl, fp64, batched=False):
+        _apply(ctx, (G, SB, block, nCB), fp64)
         ctx.restore()
         ctx.measure(parms)  # warm-up
         ctx.reset_kernel_times()
@@ -107,12 +122,11 @@ def tune_context(ctx, parms, precision: str, reps: int = 1, use_cache: bool = Tr
         for _ in range(reps):
             ctx.restore()
             ctx.measure(parms)
-        ms, n = ctx.kernel_time("contract")
+        t = sum(ctx.kernel_time(s)[0] for s in LOOP_SCOPES) / max(1, reps)
         ctx.set_profiling(False)
-        t = ms / max(1, n)
         if t < best_t:
             best, best_t = (G, SB, block, nCB), t
-    _apply(ctx, best)
+    _apply(ctx, best, fp64)
     ctx.restore()
     _store(key, best)
     return best
@@ -149,13 +163,15 @@ def tune_batch(batch, reps: int = 1, use_cache: bool = True) -> Shape:
     return best
 
 
-def _form(G: int, SB: int) -> int:
-    """kernel form of a context shape: 2 for G = 6, 3 for SB = 1 or 2, 9 for
-    SB = 9, and for SB = 0 the library's default fourth-form member (0 =
-    automatic)"""
-    if SB == 9:
-        return 9
-    return 2 if G > 4 else (0 if SB == 0 else 3)
+def _form(G: int, SB: int, fp64: bool) -> int:
+    """kernel form of a context shape: 11 for SB = 11, 9 for SB = 9, 2 for
+    G = 6, 3 for SB = 1 or 2, and for SB = 0 the default carried-line form of
+    the precision (7 FP64, 10 mixed)"""
+    if SB in (9, 11):
+        return SB
+    if G > 4:
+        return 2
+    return (7 if fp64 else 10) if SB == 0 else 3
 
 
 def _as_batch(shape: Shape):

@@ -31,7 +31,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin", HOST_CXX,
            "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"] + ARCH
 
-CU_SOURCES = ["ctx.cu", "smear.cu", "loops.cu", "layout.cu", "gen_dev.cu", "batch.cu", "noalloc.cu", "symm.cu"]
+CU_SOURCES = ["ctx.cu", "smear.cu", "loops.cu", "layout.cu", "gen_dev.cu", "batch.cu", "noalloc.cu", "symm.cu", "gram.cu"]
 CXX_SOURCES = ["gen_host.cpp", "legacy.cpp", "serve.cpp", "datfile.cpp", "cnfg.cpp"]
 
 

@@ -64,7 +64,13 @@ struct wlg_ctx {
   cudaStream_t st = nullptr;
   DevBuf U, U0, bar, til, apeA, apeB, dl, levels, lines, lines2, partial, wl, plaq_part, plaq_out,
       staging, ipt;
+  // the temporal-gauge form: g, H^-1, recursion links, B and A lines, the
+  // unitarity deviation of g
+  DevBuf gG, gH, gUh, gB, gA, gDev;
   void* lines_at = nullptr;  // buffer holding the lines of length lines_len
+  // after a temporal-gauge measurement the lines of length lines_lazy are
+  // rebuilt from the level store when they are asked for
+  int lines_lazy = 0;
   // prefetch: the next field's host-to-device copy on its own stream
   DevBuf prefetch_buf;
   cudaStream_t cst = nullptr;
@@ -337,6 +343,7 @@ static int do_smear(wlg_ctx* c, const wlg_wloop_parms* p, double* plaq) {
   if (ensure(c->levels, f3 * msl) || ensure(c->apeA, f3) || ensure(c->apeB, f3)) return -1;
   if (ensure(c->plaq_out, sizeof(double) * WLG_MAX_SM_LEVELS)) return -1;
   c->last_msl = msl;
+  c->lines_lazy = 0;  // lines of an earlier measurement no longer match the levels
   Links<T> U = view4<T>(c->U.p, g.vol);
   Links<T> A = view3<T>(c->apeA.p, g.vol), B = view3<T>(c->apeB.p, g.vol);
   Links<T> cur = U;
@@ -369,6 +376,73 @@ static int do_smear(wlg_ctx* c, const wlg_wloop_parms* p, double* plaq) {
   return 0;
 }
 
+// wloops() in the temporal gauge (gram.cu): the gauge field and H^-1 once,
+// then the first lines; per R the line step, the banded Gram product and its
+// reduction.  Returns 1 (nothing done) when the form does not apply: shapes
+// that do not fit, or a gauge field too far from unitary (links smeared
+// without projection), which the other forms then measure.
+template <class T>
+static int do_loops_gram(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
+  typedef typename V2<T>::t T2;
+  const Geo& g = c->g;
+  const int msl = p->msl;
+  GramPlan gp;
+  if (!gram_plan(gp, g, c->bc, msl, p->mwlt, c->prec == WLG_FP64)) return 1;
+  const size_t nb = gp.A * sizeof(T) * 3 * msl, na = gp.Aa * sizeof(T) * 3 * msl;
+  const size_t nwl = (size_t)msl * msl * p->mwlt * p->mwlr * g.n[0];
+  if (ensure(c->gG, gp.A * sizeof(double)) || ensure(c->gH, gp.A * sizeof(double)) ||
+      ensure(c->gDev, sizeof(unsigned long long)))
+    return -1;
+  Links<T> U = view4<T>(c->U.p, g.vol);
+  double dev = 0.0;
+  {
+    ProfScope ps(c, "gauge");
+    gauge_chain<T>(g, gp, U.p[0], (double*)c->gG.p, (double*)c->gH.p,
+                   (unsigned long long*)c->gDev.p, c->st);
+    unsigned long long bits = 0;
+    WLG_CUDA(cudaMemcpyAsync(&bits, c->gDev.p, sizeof(bits), cudaMemcpyDeviceToHost, c->st));
+    WLG_CUDA(cudaStreamSynchronize(c->st));
+    memcpy(&dev, &bits, sizeof(dev));
+  }
+  if (!(dev <= 0.25)) return 1;
+  if (ensure(c->gUh, nb) || ensure(c->gB, nb) || ensure(c->gA, na) ||
+      ensure(c->partial, gp.partial_elems * sizeof(T)) || ensure(c->wl, sizeof(double) * nwl))
+    return -1;
+  c->used_variant = 11;
+  c->lines_len = 0;
+  c->lines_at = nullptr;
+  c->lines_lazy = p->mwlr >= 2 ? p->mwlr : 0;
+  T* uh = (T*)c->gUh.p;
+  T* bl = (T*)c->gB.p;
+  T* al = (T*)c->gA.p;
+  const double* hinv = (const double*)c->gH.p;
+  {
+    ProfScope ps(c, "gauge");
+    gauge_first<T>(g, gp, msl, (const T2*)c->levels.p, (const double*)c->gG.p, hinv, uh, bl, al,
+                   c->st);
+  }
+  for (int r = 0; r < p->mwlr; r++) {
+    const int R = r + 1;
+    if (R >= 2) {
+      ProfScope ps(c, "lines");
+      gram_line_step<T>(g, gp, msl, R, uh, hinv, bl, al, c->st);
+    }
+    {
+      ProfScope ps(c, "contract");
+      gram_contract<T>(g, gp, p->mwlt, al, bl, (T*)c->partial.p, c->st);
+    }
+    {
+      ProfScope ps(c, "reduce");
+      gram_reduce<T>(g, gp, c->bc, p->mwlt, p->mwlr, r, (const T*)c->partial.p, (double*)c->wl.p,
+                     c->st);
+    }
+  }
+  if (get_error()[0]) return -1;
+  if (wl_mat)
+    WLG_CUDA(cudaMemcpyAsync(wl_mat, c->wl.p, sizeof(double) * nwl, cudaMemcpyDeviceToHost, c->st));
+  return 0;
+}
+
 // wloops(): spatial lines, fused temporal lines + contraction, reduction
 // (wloop.c:524-608); needs the level store of do_smear.
 template <class T>
@@ -388,6 +462,14 @@ static int do_loops(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
     }
     contract9_plan(cp, g, msl, p->mwlt);
   }
+  // the temporal-gauge form unless another form is asked for
+  if (c->cVariant == 0 || c->cVariant == 11) {
+    const int rc = do_loops_gram<T>(c, p, wl_mat);
+    if (rc != 1) return rc;
+    if (cp.variant == 11) cp = contract_plan(g, msl, p->mwlt, c->prec == WLG_FP64, c->cG, c->cNCB,
+                                             c->cBlock);
+  }
+  c->lines_lazy = 0;
   c->used_variant = cp.variant;
   size_t nwl = (size_t)msl * msl * p->mwlt * p->mwlr * g.n[0];
   if (ensure(c->partial, sizeof(double) * cp.partial_doubles) || ensure(c->wl, sizeof(double) * nwl))
@@ -528,8 +610,15 @@ int wlg_free_scratch(wlg_ctx* c) {
   release(c->levels);
   release(c->lines);
   release(c->lines2);
+  release(c->gG);
+  release(c->gH);
+  release(c->gUh);
+  release(c->gB);
+  release(c->gA);
+  release(c->gDev);
   c->lines_at = nullptr;
   c->lines_len = 0;
+  c->lines_lazy = 0;
   release(c->partial);
   release(c->staging);
   return 0;
@@ -542,7 +631,7 @@ int wlg_destroy(wlg_ctx* c) {
   if (c->cst) cudaStreamSynchronize(c->cst);
   harvest(c);
   DevBuf* all[] = {&c->U, &c->U0, &c->bar, &c->til, &c->apeA, &c->apeB, &c->dl, &c->levels, &c->lines, &c->lines2,
-                   &c->partial, &c->wl, &c->plaq_part, &c->plaq_out, &c->staging, &c->ipt,
+                   &c->gG, &c->gH, &c->gUh, &c->gB, &c->gA, &c->gDev, &c->partial, &c->wl, &c->plaq_part, &c->plaq_out, &c->staging, &c->ipt,
                    &c->prefetch_buf};
   for (DevBuf* b : all) release(*b);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
@@ -855,8 +944,30 @@ int wlg_download_level(wlg_ctx* c, int sl, double* aos3) {
   return download_spatial(c, (char*)c->levels.p + field_bytes(c, 3) * sl, aos3);
 }
 
+}  // extern "C"
+
+// the untransformed lines of length lines_lazy, rebuilt from the level store
+// (the temporal-gauge form keeps only gauge-transformed lines)
+template <class T> static int rebuild_lines(wlg_ctx* c) {
+  typedef typename V2<T>::t T2;
+  if (ensure(c->lines, field_bytes(c, 3) * c->last_msl)) return -1;
+  const T2* lev = (const T2*)c->levels.p;
+  T2* lines = (T2*)c->lines.p;
+  for (int R = 2; R <= c->lines_lazy; R++)
+    line_step<T>(c->g, c->last_msl, R, lev, R == 2 ? lev : lines, lines, c->st);
+  c->lines_at = lines;
+  c->lines_len = c->lines_lazy;
+  c->lines_lazy = 0;
+  return finish("download_lines");
+}
+
+extern "C" {
+
 int wlg_download_lines(wlg_ctx* c, int sl, double* aos3, int* length) {
   CTX_BEGIN(c);
+  if (!c->lines_at && c->lines_lazy >= 2 && c->levels.p) {
+    if ((c->prec == WLG_FP64 ? rebuild_lines<double>(c) : rebuild_lines<float>(c)) != 0) return -1;
+  }
   if (length) *length = c->lines_len;
   if (!c->lines_at || c->lines_len < 2 || sl < 0 || sl >= c->last_msl) {
     set_error("no spatial lines of level %d", sl);
@@ -982,7 +1093,7 @@ int wlg_reset_kernel_times(wlg_ctx* c) {
 
 int wlg_set_contract_tuning(wlg_ctx* c, int variant, int G, int SB, int nCB, int block) {
   CTX_BEGIN(c);
-  if (variant == 1 || variant < 0 || variant > 10 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
+  if (variant == 1 || variant < 0 || variant > 11 || G < 0 || G == 5 || G > 6 || SB < 0 || SB > 2 ||
       nCB < 0 || (block != 0 && (block % 32 != 0 || block > 128)) ||
       (variant == 2 && G == 6 && SB == 2) || (variant >= 3 && G > 4)) {
     set_error("bad contraction tuning (variant %d, G %d, SB %d, nCB %d, block %d)", variant, G,
@@ -1010,6 +1121,16 @@ int wlg_set_contract_shape(wlg_ctx* c, int G, int nCB, int block) {
 }
 
 void* wlg_stream(wlg_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+int wlg_contract_form(wlg_ctx* c, int* form) {
+  CTX_BEGIN(c);
+  if (!form) {
+    set_error("null argument");
+    return -1;
+  }
+  *form = c->used_variant;
+  return 0;
+}
 
 long long wlg_launch_count(void) { return g_launches.load(); }
 

@@ -121,6 +121,47 @@ int wait_selftest(double limit_s, int* timed_out, double* elapsed_s);
 void contract_reduce(const Geo& g, const ContractPlan& p, int msl, int mwlt, int mwlr, int r,
                      const double* partial, double* wl_mat, cudaStream_t st);
 
+// ---- the temporal-gauge Gram form (gram.cu) -----------------------------------
+// Shapes of one lattice's Gram stage; gram_plan returns false when the level
+// count or mwlt do not fit the kernel (the other forms then apply).
+struct GramPlan {
+  int esize = 0;    // element bytes (4: mixed, 8: FP64)
+  int L = 0;        // levels
+  int Nu = 0;       // unrolled time extent (N0 + mwlt periodic, N0 open)
+  int ntile = 0;    // 32-site tiles per time slice
+  size_t A = 0;     // elements of one slab array over Nu slices
+  size_t Aa = 0;    // elements of one slab array over N0 slices (the A lines)
+  int TQ = 0, NG = 0, BX = 0, NYB = 0, nblk = 0, nrows = 0, stages = 0, block = 0;
+  size_t smem = 0;  // dynamic shared memory per block
+  int nchunks = 0, cpc = 0, nsplit = 0;
+  size_t partial_elems = 0;
+};
+bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64);
+// The gauge field g and H^-1 = (g g^dag)^-1 (FP64 slabs of A doubles each)
+// from the temporal links u0; *dev (device) receives max |g g^dag - 1| as the
+// bits of a non-negative double (the form is not used when it exceeds 1/4).
+template <class T>
+void gauge_chain(const Geo& g, const GramPlan& p, const typename V2<T>::t* u0, double* G,
+                 double* Hinv, unsigned long long* dev, cudaStream_t st);
+// The recursion links uh and the lines of length 1 (blines, alines; [msl][3]
+// slab arrays of A resp. Aa elements) from the level store.
+template <class T>
+void gauge_first(const Geo& g, const GramPlan& p, int msl, const typename V2<T>::t* levels,
+                 const double* G, const double* Hinv, T* uh, T* blines, T* alines,
+                 cudaStream_t st);
+// blines of length R from those of length R-1 (in place), alines of length R
+template <class T>
+void gram_line_step(const Geo& g, const GramPlan& p, int msl, int R, const T* uh,
+                    const double* Hinv, T* blines, T* alines, cudaStream_t st);
+// partial[nsplit][N0][mwlt][L][L] of the lines of one R
+template <class T>
+void gram_contract(const Geo& g, const GramPlan& p, int mwlt, const T* alines, const T* blines,
+                   T* partial, cudaStream_t st);
+// wl_mat entries of spatial extent index r from the partials
+template <class T>
+void gram_reduce(const Geo& g, const GramPlan& p, int bc, int mwlt, int mwlr, int r,
+                 const T* partial, double* wl, cudaStream_t st);
+
 // ---- batched stages (one launch over many lattices) ------------------------
 // A: device array of n per-lattice argument records; pre: device array of
 // n+1 prefix sums of the per-lattice work items (blocks for the contraction).
