@@ -91,12 +91,15 @@ def test_several_blocks_and_splits(wide, prec):
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_unprojected_field_falls_back(prec):
-    """Links at half the norm of SU(3) matrices, smeared without projection:
-    g g^dag drifts far from 1 along time, so the carried-line form measures
-    (and still agrees with the oracle)."""
+    """Links at 0.85 of the norm of SU(3) matrices, smeared without
+    projection (weak HYP weights, so the loops stay of order 1e-4 to 0.3):
+    g g^dag is far from 1 already on the second slice (|g g^dag - 1| about
+    0.5), so the carried-line form measures (and still agrees with the
+    oracle)."""
     n, bc = (8, 4, 4, 4), 3
-    p = WloopParms(msl=2, nss=[0, 1], mwlt=4, mwlr=2, op_smear=APE, alpha_ape=0.5, proj_iter=0)
-    u = 0.5 * generate_links(n, bc, 940, 0.3)
+    p = WloopParms(msl=2, nss=[0, 1], mwlt=4, mwlr=2, op_smear=APE, alpha_ape=0.5, proj_iter=0,
+                   alpha_action=(0.2, 0.2, 0.2))
+    u = 0.85 * generate_links(n, bc, 940, 0.3)
     uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
     ref, ref_abs = O.wloop_sum(n, bc, uh, p, want_abs=True)
     with Context(n, bc, prec) as c:
@@ -106,7 +109,7 @@ def test_unprojected_field_falls_back(prec):
     if prec == "fp64":
         assert_wl_close(got, ref, ref_abs)
     else:
-        # loops of links at half norm are small and cancel: scaled bar
+        # loops of shrunken links are small and cancel: scaled bar
         nz = ref != 0.0
         err = np.abs(got - ref)[nz] / np.maximum(np.abs(ref), ref_abs)[nz]
         assert err.max() <= 1e-6

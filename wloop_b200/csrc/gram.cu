@@ -43,6 +43,7 @@
 // thousand products) and the per-block partial sums are added in FP64 in a
 // fixed order.
 #include <algorithm>
+#include <cmath>
 
 #include "internal.h"
 
@@ -257,15 +258,19 @@ __global__ void __launch_bounds__(128) k_gauge_line_step(Geo g, int Nu, int ntil
                                                          E* __restrict__ blines,
                                                          E* __restrict__ alines, size_t A,
                                                          size_t Aa) {
-  const long long n = (long long)msl * 3 * Nu * ntile * 32;
+  // item order (y0, tile, level x direction, lane): the 3 msl arrays of one
+  // tile run in neighbouring warps, so the two H^-1 tiles they share come
+  // from L2 rather than once per array from DRAM
+  const int nq = msl * 3;
+  const long long n = (long long)nq * Nu * ntile * 32;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n;
        w += (long long)gridDim.x * blockDim.x) {
     const int lane = (int)(w & 31);
     long long rest = w >> 5;
+    const int q = (int)(rest % nq);  // sl * 3 + k
+    rest /= nq;
     const int jt = (int)(rest % ntile);
-    rest /= ntile;
-    const int y0 = (int)(rest % Nu);
-    const int q = (int)(rest / Nu);  // sl * 3 + k
+    const int y0 = (int)(rest / ntile);
     const int k = q % 3;
     const int j = jt * 32 + lane;
     const size_t tile = slab_tile(y0, ntile, jt);
@@ -298,14 +303,17 @@ __global__ void __launch_bounds__(128) k_gauge_line_step(Geo g, int Nu, int ntil
 // consecutive slab elements of one direction (32 sites x 1 component in FP32,
 // 16 in FP64, 128 bytes).  Per chunk the block stages its A rows (sl, x0) and
 // its B rows (sl, y0), y0 in [blk*BX + 1, blk*BX + BX + mwlt), into shared
-// memory with cp.async (16 bytes per copy; rows of 144 bytes, 128 of data and
-// 16 of padding, so that rows eight apart fall on different banks), `stages`
-// chunks ahead of the arithmetic.  Thread (i, gq) owns start slice
-// x0 = blk*BX + i and the TQ extents T = gq + 1 + NG j (j < TQ): per 16-byte
-// column group it reads the L A-vectors of its slice and the L B-vectors of
-// each partner slice and accumulates TQ L^2 dot products in registers.
-// Lanes of a warp share start slices (broadcast reads), and the partner rows
-// one read of a warp touches span at most 32/NG + NG - 1 consecutive slices.
+// memory with cp.async, `stages` chunks ahead of the arithmetic.  A staged
+// row is 128 bytes, its 16-byte slot q stored at q ^ (row & 7) so that eight
+// consecutive rows read at one slot fall on distinct banks; each level's rows
+// start at a multiple of 8 (A rows BXp apart, B rows NYBp apart), so a
+// thread's swizzle is fixed.  Thread (i, gq) owns start slice x0 = blk*BX + i
+// and the TQ extents T = gq + 1 + NG j (j < TQ): per 16-byte column group it
+// reads the L A-vectors of its slice and the L B-vectors of each partner slice
+// and advances its TQ L^2 sums one component at a time (L^2 independent FMAs
+// between two updates of one sum).  Lanes of a warp share start slices
+// (broadcast reads), and the partner rows one read of a warp touches span at
+// most 32/NG + NG - 1 consecutive slices.
 // ---------------------------------------------------------------------------
 template <class E> struct GVec;
 template <> struct GVec<float> {
@@ -316,17 +324,10 @@ template <> struct GVec<double> {
   typedef double2 t;
   enum { N = 2 };
 };
-
-__device__ __forceinline__ float dot_acc(float acc, const float4& a, const float4& b) {
-  acc = fmaf(a.x, b.x, acc);
-  acc = fmaf(a.y, b.y, acc);
-  acc = fmaf(a.z, b.z, acc);
-  return fmaf(a.w, b.w, acc);
+__device__ __forceinline__ float comp(const float4& v, int c) {
+  return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
 }
-__device__ __forceinline__ double dot_acc(double acc, const double2& a, const double2& b) {
-  acc = fma(a.x, b.x, acc);
-  return fma(a.y, b.y, acc);
-}
+__device__ __forceinline__ double comp(const double2& v, int c) { return c == 0 ? v.x : v.y; }
 
 __device__ __forceinline__ void gcp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -343,7 +344,7 @@ __device__ __forceinline__ void gcp_wait(int n) {
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-constexpr int kRowBytes = 144;
+constexpr int kRowBytes = 128;
 constexpr int kMaxGramThreads = 256;
 
 struct GramArgs {
@@ -351,10 +352,11 @@ struct GramArgs {
   const void* blines;  // [msl][3] slab arrays of A elements (Nu slices)
   void* partial;       // [nsplit][N0][mwlt][L][L] partial sums (element type of the form)
   size_t A, Aa;
-  int Nu, ntile, N0, mwlt, BX, NG, NYB, nblk, nchunks, cpc, stages, nrows;
+  int Nu, ntile, N0, mwlt, BX, BXp, NG, NYB, NYBp, nblk, nchunks, cpc, stages, nrows;
 };
 
 __host__ __device__ __forceinline__ int gram_tab_bytes(int nrows) { return (nrows * 8 + 127) & ~127; }
+__host__ __device__ __forceinline__ int round8(int v) { return (v + 7) & ~7; }
 
 template <class E, int L, int TQ>
 __global__ void __launch_bounds__(kMaxGramThreads, 1) k_gram(GramArgs P) {
@@ -368,18 +370,18 @@ __global__ void __launch_bounds__(kMaxGramThreads, 1) k_gram(GramArgs P) {
   const int c0 = split * P.cpc;
   const int nk = min(P.nchunks, c0 + P.cpc) - c0;
   const size_t stage_bytes = (size_t)P.nrows * kRowBytes;
-  const int nA = L * P.BX;  // rows [0, nA): A rows (sl, x0); then B rows (sl, y0)
+  const int nA = L * P.BXp;  // rows [0, nA): A rows (sl, x0); then B rows (sl, y0)
   const size_t tile_bytes = (size_t)P.ntile * kSlabTile * sizeof(E);
   for (int r = threadIdx.x; r < P.nrows; r += blockDim.x) {
-    const char* ptr = nullptr;
+    const char* ptr = nullptr;  // padding rows and rows past the lattice stay unloaded
     if (r < nA) {
-      const int sl = r / P.BX, y0 = blk * P.BX + (r - sl * P.BX);
-      if (y0 < P.N0)
+      const int sl = r / P.BXp, ii = r - sl * P.BXp, y0 = blk * P.BX + ii;
+      if (ii < P.BX && y0 < P.N0)
         ptr = static_cast<const char*>(P.alines) + (size_t)(sl * 3) * P.Aa * sizeof(E) +
               (size_t)y0 * tile_bytes;
     } else {
-      const int rr = r - nA, sl = rr / P.NYB, y0 = blk * P.BX + 1 + (rr - sl * P.NYB);
-      if (y0 < P.Nu)
+      const int rr = r - nA, sl = rr / P.NYBp, yy = rr - sl * P.NYBp, y0 = blk * P.BX + 1 + yy;
+      if (yy < P.NYB && y0 < P.Nu)
         ptr = static_cast<const char*>(P.blines) + (size_t)(sl * 3) * P.A * sizeof(E) +
               (size_t)y0 * tile_bytes;
     }
@@ -397,7 +399,9 @@ __global__ void __launch_bounds__(kMaxGramThreads, 1) k_gram(GramArgs P) {
     for (int p = threadIdx.x; p < npieces; p += blockDim.x) {
       const int r = p >> 3, q = p & 7;
       const char* ro = rowtab[r];
-      if (ro) gcp_async16(dst + r * kRowBytes + q * 16, ro + (r < nA ? offA : offB) + q * 16);
+      if (ro)
+        gcp_async16(dst + r * kRowBytes + ((q ^ (r & 7)) << 4),
+                    ro + (r < nA ? offA : offB) + q * 16);
     }
   };
 
@@ -406,12 +410,14 @@ __global__ void __launch_bounds__(kMaxGramThreads, 1) k_gram(GramArgs P) {
   const int x0 = blk * P.BX + i;
   const bool live = (i < P.BX) && (x0 < P.N0);
   if (i >= P.BX) i = P.BX - 1;  // idle threads read in-range rows and store nothing
-  int trow[TQ];
+  const int sa = i & 7;         // swizzle of this thread's A rows
+  int brow[TQ], sb[TQ];
 #pragma unroll
   for (int j = 0; j < TQ; j++) {
     int T = gq + 1 + P.NG * j;
     if (T > P.mwlt) T = P.mwlt;
-    trow[j] = nA + i + T - 1;
+    brow[j] = nA + i + T - 1;
+    sb[j] = (i + T - 1) & 7;
   }
   E acc[TQ][L][L];
 #pragma unroll
@@ -425,7 +431,7 @@ __global__ void __launch_bounds__(kMaxGramThreads, 1) k_gram(GramArgs P) {
     if (s < nk) issue(c0 + s, s);
     gcp_commit();
   }
-  const size_t astride = (size_t)P.BX * kRowBytes, bstride = (size_t)P.NYB * kRowBytes;
+  const size_t astride = (size_t)P.BXp * kRowBytes, bstride = (size_t)P.NYBp * kRowBytes;
   for (int it = 0; it < nk; it++) {
     gcp_wait(P.stages - 2);
     __syncthreads();
@@ -437,20 +443,24 @@ __global__ void __launch_bounds__(kMaxGramThreads, 1) k_gram(GramArgs P) {
     const unsigned char* st = stage0 + (size_t)(it % P.stages) * stage_bytes;
     const unsigned char* arow = st + (size_t)i * kRowBytes;
 #pragma unroll 1
-    for (int kk = 0; kk < KW; kk += VN) {
+    for (int qk = 0; qk < 8; qk++) {  // 16-byte column groups of the chunk
       V a[L];
 #pragma unroll
       for (int s1 = 0; s1 < L; s1++)
-        a[s1] = *reinterpret_cast<const V*>(arow + s1 * astride + kk * sizeof(E));
+        a[s1] = *reinterpret_cast<const V*>(arow + s1 * astride + ((qk ^ sa) << 4));
 #pragma unroll
       for (int j = 0; j < TQ; j++) {
-        const unsigned char* brow = st + (size_t)trow[j] * kRowBytes + kk * sizeof(E);
+        const unsigned char* bp = st + (size_t)brow[j] * kRowBytes + ((qk ^ sb[j]) << 4);
+        V b[L];
 #pragma unroll
-        for (int s2 = 0; s2 < L; s2++) {
-          const V b = *reinterpret_cast<const V*>(brow + s2 * bstride);
+        for (int s2 = 0; s2 < L; s2++) b[s2] = *reinterpret_cast<const V*>(bp + s2 * bstride);
 #pragma unroll
-          for (int s1 = 0; s1 < L; s1++) acc[j][s1][s2] = dot_acc(acc[j][s1][s2], a[s1], b);
-        }
+        for (int c = 0; c < VN; c++)
+#pragma unroll
+          for (int s1 = 0; s1 < L; s1++)
+#pragma unroll
+            for (int s2 = 0; s2 < L; s2++)
+              acc[j][s1][s2] = fma(comp(a[s1], c), comp(b[s2], c), acc[j][s1][s2]);
       }
     }
   }
@@ -562,12 +572,14 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64) 
   // the fewest start-slice blocks whose rows fit two stages
   for (int nblk = (N0 + bxmax - 1) / bxmax; nblk <= N0; nblk++) {
     const int BX = (N0 + nblk - 1) / nblk;
-    const int nrows = msl * (2 * BX + mwlt - 1);
+    const int nrows = msl * (round8(BX) + round8(BX + mwlt - 1));
     const size_t tab = (size_t)gram_tab_bytes(nrows), per = (size_t)nrows * kRowBytes;
     if (tab + 2 * per > smem_max) continue;
     p.BX = BX;
+    p.BXp = round8(BX);
     p.nblk = (N0 + BX - 1) / BX;
     p.NYB = BX + mwlt - 1;
+    p.NYBp = round8(p.NYB);
     p.nrows = nrows;
     p.stages = (int)std::min<size_t>(4, (smem_max - tab) / per);
     p.smem = tab + (size_t)p.stages * per;
@@ -582,6 +594,15 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64) 
   long long cpc = ((long long)p.nchunks * p.nblk + target - 1) / target;
   if (cpc < 32) cpc = 32;
   if (cpc > 512) cpc = 512;
+  if (!fp64) {
+    // FP32 sums: the rounding error of one partial grows with its run of
+    // n = cpc x 32 products, and the relative error of W after the FP64
+    // sum of the partials as n / sqrt(all products); a run of at most
+    // sqrt(nchunks / 32) chunks keeps it at the level of the full-size
+    // lattices, whose runs are short against their column count
+    const long long acc_cap = (long long)std::sqrt((double)p.nchunks / 32.0);
+    cpc = std::max(1LL, std::min(cpc, acc_cap));
+  }
   p.cpc = (int)cpc;
   p.nsplit = (p.nchunks + p.cpc - 1) / p.cpc;
   p.partial_elems = (size_t)p.nsplit * N0 * mwlt * msl * msl;
@@ -635,8 +656,10 @@ void gram_contract(const Geo& g, const GramPlan& p, int mwlt, const T* alines, c
   a.N0 = g.n[0];
   a.mwlt = mwlt;
   a.BX = p.BX;
+  a.BXp = p.BXp;
   a.NG = p.NG;
   a.NYB = p.NYB;
+  a.NYBp = p.NYBp;
   a.nblk = p.nblk;
   a.nchunks = p.nchunks;
   a.cpc = p.cpc;

@@ -131,7 +131,8 @@ struct GramPlan {
   int ntile = 0;    // 32-site tiles per time slice
   size_t A = 0;     // elements of one slab array over Nu slices
   size_t Aa = 0;    // elements of one slab array over N0 slices (the A lines)
-  int TQ = 0, NG = 0, BX = 0, NYB = 0, nblk = 0, nrows = 0, stages = 0, block = 0;
+  int TQ = 0, NG = 0, BX = 0, BXp = 0, NYB = 0, NYBp = 0, nblk = 0, nrows = 0, stages = 0;
+  int block = 0;
   size_t smem = 0;  // dynamic shared memory per block
   int nchunks = 0, cpc = 0, nsplit = 0;
   size_t partial_elems = 0;
