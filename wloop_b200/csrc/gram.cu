@@ -309,9 +309,11 @@ __global__ void __launch_bounds__(128) k_gauge_line_step(Geo g, int Nu, int ntil
 // start at a multiple of 8 (A rows BXp apart, B rows NYBp apart), so a
 // thread's swizzle is fixed.  Thread (i, gq) owns start slice x0 = blk*BX + i
 // and the TQ extents T = gq + 1 + NG j (j < TQ): per 16-byte column group it
-// reads the L A-vectors of its slice and the L B-vectors of each partner slice
-// and advances its TQ L^2 sums one component at a time (L^2 independent FMAs
-// between two updates of one sum).  Lanes of a warp share start slices
+// reads the L A-vectors of its slice and, one at a time, the L B-vectors of
+// each partner slice, advancing the L sums of a B vector one component at a
+// time (L independent FMAs between two updates of one sum).  At most 192
+// threads and 170 registers a thread, so two blocks share an SM and one
+// computes while the other waits at its barrier.  Lanes of a warp share start slices
 // (broadcast reads), and the partner rows one read of a warp touches span at
 // most 32/NG + NG - 1 consecutive slices.
 // ---------------------------------------------------------------------------
@@ -345,7 +347,8 @@ __device__ __forceinline__ void gcp_wait(int n) {
 }
 
 constexpr int kRowBytes = 128;
-constexpr int kMaxGramThreads = 256;
+constexpr int kMaxGramThreads = 192;  // two blocks per SM: at most 170 registers a thread
+constexpr unsigned kNoRow = 0xffffffffu;
 
 struct GramArgs {
   const void* alines;  // [msl][3] slab arrays of Aa elements (N0 slices)
@@ -355,16 +358,18 @@ struct GramArgs {
   int Nu, ntile, N0, mwlt, BX, BXp, NG, NYB, NYBp, nblk, nchunks, cpc, stages, nrows;
 };
 
-__host__ __device__ __forceinline__ int gram_tab_bytes(int nrows) { return (nrows * 8 + 127) & ~127; }
+__host__ __device__ __forceinline__ int gram_tab_bytes(int nrows) { return (nrows * 4 + 127) & ~127; }
 __host__ __device__ __forceinline__ int round8(int v) { return (v + 7) & ~7; }
 
 template <class E, int L, int TQ>
-__global__ void __launch_bounds__(kMaxGramThreads, 1) k_gram(GramArgs P) {
+__global__ void __launch_bounds__(kMaxGramThreads, 2) k_gram(GramArgs P) {
   constexpr int KW = 128 / (int)sizeof(E);
   constexpr int VN = GVec<E>::N;
   typedef typename GVec<E>::t V;
   extern __shared__ __align__(128) unsigned char gsm[];
-  const char** rowtab = reinterpret_cast<const char**>(gsm);
+  // row table: offset of row r's slice in 16-byte units from the A (r < nA)
+  // or the B lines, kNoRow for rows not loaded
+  unsigned* rowtab = reinterpret_cast<unsigned*>(gsm);
   unsigned char* stage0 = gsm + gram_tab_bytes(P.nrows);
   const int blk = blockIdx.x % P.nblk, split = blockIdx.x / P.nblk;
   const int c0 = split * P.cpc;
@@ -373,19 +378,17 @@ __global__ void __launch_bounds__(kMaxGramThreads, 1) k_gram(GramArgs P) {
   const int nA = L * P.BXp;  // rows [0, nA): A rows (sl, x0); then B rows (sl, y0)
   const size_t tile_bytes = (size_t)P.ntile * kSlabTile * sizeof(E);
   for (int r = threadIdx.x; r < P.nrows; r += blockDim.x) {
-    const char* ptr = nullptr;  // padding rows and rows past the lattice stay unloaded
+    unsigned off = kNoRow;  // padding rows and rows past the lattice stay unloaded
     if (r < nA) {
       const int sl = r / P.BXp, ii = r - sl * P.BXp, y0 = blk * P.BX + ii;
       if (ii < P.BX && y0 < P.N0)
-        ptr = static_cast<const char*>(P.alines) + (size_t)(sl * 3) * P.Aa * sizeof(E) +
-              (size_t)y0 * tile_bytes;
+        off = (unsigned)(((size_t)(sl * 3) * P.Aa * sizeof(E) + (size_t)y0 * tile_bytes) >> 4);
     } else {
       const int rr = r - nA, sl = rr / P.NYBp, yy = rr - sl * P.NYBp, y0 = blk * P.BX + 1 + yy;
       if (yy < P.NYB && y0 < P.Nu)
-        ptr = static_cast<const char*>(P.blines) + (size_t)(sl * 3) * P.A * sizeof(E) +
-              (size_t)y0 * tile_bytes;
+        off = (unsigned)(((size_t)(sl * 3) * P.A * sizeof(E) + (size_t)y0 * tile_bytes) >> 4);
     }
-    rowtab[r] = ptr;
+    rowtab[r] = off;
   }
   __syncthreads();
   const int per_dir = P.ntile * 18 * (32 / KW);
@@ -393,15 +396,15 @@ __global__ void __launch_bounds__(kMaxGramThreads, 1) k_gram(GramArgs P) {
   auto issue = [&](int cidx, int buf) {
     const int k = cidx / per_dir;
     const size_t within = (size_t)(cidx - k * per_dir) * KW;
-    const size_t offA = ((size_t)k * P.Aa + within) * sizeof(E);
-    const size_t offB = ((size_t)k * P.A + within) * sizeof(E);
+    const char* baseA = static_cast<const char*>(P.alines) + ((size_t)k * P.Aa + within) * sizeof(E);
+    const char* baseB = static_cast<const char*>(P.blines) + ((size_t)k * P.A + within) * sizeof(E);
     unsigned char* dst = stage0 + (size_t)buf * stage_bytes;
     for (int p = threadIdx.x; p < npieces; p += blockDim.x) {
       const int r = p >> 3, q = p & 7;
-      const char* ro = rowtab[r];
-      if (ro)
+      const unsigned ro = rowtab[r];
+      if (ro != kNoRow)
         gcp_async16(dst + r * kRowBytes + ((q ^ (r & 7)) << 4),
-                    ro + (r < nA ? offA : offB) + q * 16);
+                    (r < nA ? baseA : baseB) + ((size_t)ro << 4) + q * 16);
     }
   };
 
@@ -451,16 +454,15 @@ __global__ void __launch_bounds__(kMaxGramThreads, 1) k_gram(GramArgs P) {
 #pragma unroll
       for (int j = 0; j < TQ; j++) {
         const unsigned char* bp = st + (size_t)brow[j] * kRowBytes + ((qk ^ sb[j]) << 4);
-        V b[L];
 #pragma unroll
-        for (int s2 = 0; s2 < L; s2++) b[s2] = *reinterpret_cast<const V*>(bp + s2 * bstride);
+        for (int s2 = 0; s2 < L; s2++) {
+          const V b = *reinterpret_cast<const V*>(bp + s2 * bstride);
 #pragma unroll
-        for (int c = 0; c < VN; c++)
+          for (int c = 0; c < VN; c++)
 #pragma unroll
-          for (int s1 = 0; s1 < L; s1++)
-#pragma unroll
-            for (int s2 = 0; s2 < L; s2++)
-              acc[j][s1][s2] = fma(comp(a[s1], c), comp(b[s2], c), acc[j][s1][s2]);
+            for (int s1 = 0; s1 < L; s1++)
+              acc[j][s1][s2] = fma(comp(a[s1], c), comp(b, c), acc[j][s1][s2]);
+        }
       }
     }
   }
@@ -505,12 +507,12 @@ __global__ void __launch_bounds__(256) k_gram_reduce(const E* __restrict__ parti
 
 // ---------------------------------------------------------------------------
 // Instantiations: (levels L, extents per thread TQ).  FP32 keeps at most
-// 108 sums per thread, FP64 at most 72 (144 registers).
+// 128 sums per thread, FP64 at most 64 (128 registers), within 170.
 // ---------------------------------------------------------------------------
 #define WLG_GRAM_F32(X) X(float, 1, 8) X(float, 2, 8) X(float, 3, 6) X(float, 4, 6) \
   X(float, 4, 4) X(float, 5, 4) X(float, 6, 3) X(float, 6, 2) X(float, 7, 2) X(float, 8, 2)
 #define WLG_GRAM_F64(X) X(double, 1, 8) X(double, 2, 6) X(double, 3, 4) X(double, 4, 3) \
-  X(double, 4, 2) X(double, 5, 2) X(double, 6, 2) X(double, 6, 1) X(double, 7, 1) X(double, 8, 1)
+  X(double, 4, 2) X(double, 5, 2) X(double, 6, 1) X(double, 7, 1) X(double, 8, 1)
 
 template <class E> struct GramKernel {
   static void* get(int L, int TQ) {
@@ -568,24 +570,30 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64) 
   if (p.NG > kMaxGramThreads) return false;
   const int N0 = g.n[0];
   const int bxmax = kMaxGramThreads / p.NG;
-  const size_t smem_max = 227 * 1024;
-  // the fewest start-slice blocks whose rows fit two stages
-  for (int nblk = (N0 + bxmax - 1) / bxmax; nblk <= N0; nblk++) {
-    const int BX = (N0 + nblk - 1) / nblk;
-    const int nrows = msl * (round8(BX) + round8(BX + mwlt - 1));
-    const size_t tab = (size_t)gram_tab_bytes(nrows), per = (size_t)nrows * kRowBytes;
-    if (tab + 2 * per > smem_max) continue;
-    p.BX = BX;
-    p.BXp = round8(BX);
-    p.nblk = (N0 + BX - 1) / BX;
-    p.NYB = BX + mwlt - 1;
-    p.NYBp = round8(p.NYB);
-    p.nrows = nrows;
-    p.stages = (int)std::min<size_t>(4, (smem_max - tab) / per);
-    p.smem = tab + (size_t)p.stages * per;
-    break;
+  // the fewest start-slice blocks whose rows fit two stages in half an SM's
+  // shared memory (two blocks per SM), else in a whole SM's
+  const size_t smem_half = 113 * 1024, smem_max = 227 * 1024;
+  for (int pass = 0; pass < 2 && p.BX == 0; pass++) {
+    const size_t lim = pass == 0 ? smem_half : smem_max;
+    for (int nblk = (N0 + bxmax - 1) / bxmax; nblk <= N0; nblk++) {
+      const int BX = (N0 + nblk - 1) / nblk;
+      const int nrows = msl * (round8(BX) + round8(BX + mwlt - 1));
+      const size_t tab = (size_t)gram_tab_bytes(nrows), per = (size_t)nrows * kRowBytes;
+      if (tab + 2 * per > lim) continue;
+      p.BX = BX;
+      p.BXp = round8(BX);
+      p.nblk = (N0 + BX - 1) / BX;
+      p.NYB = BX + mwlt - 1;
+      p.NYBp = round8(p.NYB);
+      p.nrows = nrows;
+      p.stages = (int)std::min<size_t>(4, (lim - tab) / per);
+      p.smem = tab + (size_t)p.stages * per;
+      break;
+    }
   }
   if (p.BX == 0) return false;
+  // row offsets are kept as 32-bit multiples of 16 bytes
+  if ((size_t)3 * msl * p.A * esz / 16 >= (size_t)kNoRow) return false;
   p.block = ((p.BX * p.NG + 31) / 32) * 32;
   p.nchunks = 3 * p.ntile * 18 * (32 * esz / 128);
   // about 16 waves of blocks, 32 to 512 chunks per block: a bounded run of
