@@ -289,6 +289,19 @@ int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
 int wlg_set_contract_tuning(wlg_ctx* ctx, int variant, int G, int SB, int nCB, int block);
 /* The contraction form the last measurement on ctx used (0: none yet). */
 int wlg_contract_form(wlg_ctx* ctx, int* form);
+/* Shape of the temporal-gauge form's Gram kernel (0: automatic): occ blocks
+ * per SM (1: one block of up to 256 threads, 2: two of up to 192), ord the
+ * order of its FMAs (1: dot-product chains, 2: one component at a time),
+ * bx an upper bound on the start slices per block, stages the copy pipeline
+ * depth (2-4), cpc the column chunks per block.  Results do not depend on
+ * occ, ord, bx or stages; cpc sets how the FP32 sums of the mixed form are
+ * split (FP32 rounding only). */
+int wlg_set_gram_tuning(wlg_ctx* ctx, int occ, int ord, int bx, int stages, int cpc);
+/* The plan those settings give for msl levels and mwlt on ctx's lattice:
+ * shape[10] = {extents per thread, occ, ord, start slices per block, blocks
+ * of start slices, stages, chunks per block, column splits, threads per
+ * block, shared memory per block in KiB}. */
+int wlg_gram_shape(wlg_ctx* ctx, int msl, int mwlt, int* shape);
 /* The context's CUDA stream (cudaStream_t), for callers that record events. */
 void* wlg_stream(wlg_ctx* ctx);
 /* Number of wloop_b200 kernel launches issued by this process so far. */

@@ -113,3 +113,29 @@ def test_unprojected_field_falls_back(prec):
         nz = ref != 0.0
         err = np.abs(got - ref)[nz] / np.maximum(np.abs(ref), ref_abs)[nz]
         assert err.max() <= 1e-6
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_kernel_variants_agree_bit_for_bit(prec):
+    """Occupancy, FMA order, start slices per block and pipeline depth change
+    neither the FMAs of a sum nor their order: the results are identical
+    (for a fixed number of column chunks per block)."""
+    n, bc, p = WIDE[0]
+    with Context(n, bc, prec) as c:
+        c.generate(950, 0.3)
+        c.snapshot()
+        c.set_gram_tuning(cpc=2)
+        ref = c.measure(p)
+        occs = (1, 2)
+        for occ in occs:
+            for ord_ in (1, 2):
+                for bx, stages in ((0, 0), (8, 2), (13, 3)):
+                    c.set_gram_tuning(occ, ord_, bx, stages, 2)
+                    try:
+                        shape = c.gram_shape(p.msl, p.mwlt)
+                    except Exception:
+                        continue  # no kernel of this occupancy for this precision and msl
+                    c.restore()
+                    got = c.measure(p)
+                    assert c.contract_form == 11
+                    assert np.array_equal(got, ref), (occ, ord_, bx, stages, shape)

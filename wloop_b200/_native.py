@@ -92,6 +92,8 @@ def _load():
         "wlg_set_contract_tuning": (i, [vp, i, i, i, i, i]),
         "wlg_stream": (vp, [vp]),
         "wlg_contract_form": (i, [vp, ip]),
+        "wlg_set_gram_tuning": (i, [vp, i, i, i, i, i]),
+        "wlg_gram_shape": (i, [vp, i, i, ip]),
         "wlg_launch_count": (C.c_longlong, []),
         "wlg_snapshot": (i, [vp]),
         "wlg_gauge_transform": (i, [vp, u64, d]),

@@ -272,6 +272,17 @@ class Context:
         check(lib.wlg_set_contract_tuning(self._h, variant, G, SB, nCB, block),
               "set_contract_tuning")
 
+    def set_gram_tuning(self, occ=0, ord=0, bx=0, stages=0, cpc=0):
+        """Shape of the temporal-gauge form's Gram kernel (0: automatic)."""
+        check(lib.wlg_set_gram_tuning(self._h, occ, ord, bx, stages, cpc), "set_gram_tuning")
+
+    def gram_shape(self, msl: int, mwlt: int) -> dict:
+        """The Gram kernel's plan for msl levels and mwlt on this lattice."""
+        v = (C.c_int * 10)()
+        check(lib.wlg_gram_shape(self._h, msl, mwlt, v), "gram_shape")
+        keys = ("tq", "occ", "ord", "bx", "nblk", "stages", "cpc", "nsplit", "block", "smem_kib")
+        return dict(zip(keys, list(v)))
+
     @property
     def contract_form(self) -> int:
         """Contraction form of the last measurement (11: temporal gauge; 0: none yet)."""

@@ -77,6 +77,7 @@ struct wlg_ctx {
   cudaEvent_t copied = nullptr, consumed = nullptr;
   bool prefetched = false;
   int cG = 0, cNCB = 0, cBlock = 0, cVariant = 0, cSB = 0;
+  GramTuning gtune;  // the temporal-gauge form's kernel variant and shape
   bool prof = false;
   std::map<std::string, ProfStat> stats;
   struct Pending {
@@ -387,7 +388,7 @@ static int do_loops_gram(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
   const Geo& g = c->g;
   const int msl = p->msl;
   GramPlan gp;
-  if (!gram_plan(gp, g, c->bc, msl, p->mwlt, c->prec == WLG_FP64)) return 1;
+  if (!gram_plan(gp, g, c->bc, msl, p->mwlt, c->prec == WLG_FP64, &c->gtune)) return 1;
   const size_t nb = gp.A * sizeof(T) * 3 * msl, na = gp.Aa * sizeof(T) * 3 * msl;
   const size_t nwl = (size_t)msl * msl * p->mwlt * p->mwlr * g.n[0];
   if (ensure(c->gG, gp.A * sizeof(double)) || ensure(c->gH, gp.A * sizeof(double)) ||
@@ -1121,6 +1122,35 @@ int wlg_set_contract_shape(wlg_ctx* c, int G, int nCB, int block) {
 }
 
 void* wlg_stream(wlg_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+int wlg_set_gram_tuning(wlg_ctx* c, int occ, int ord, int bx, int stages, int cpc) {
+  CTX_BEGIN(c);
+  if (occ < 0 || occ > 2 || ord < 0 || ord > 2 || bx < 0 || stages < 0 || stages > 4 ||
+      stages == 1 || cpc < 0) {
+    set_error("bad temporal-gauge tuning (occ %d, ord %d, bx %d, stages %d, cpc %d)", occ, ord,
+              bx, stages, cpc);
+    return -1;
+  }
+  c->gtune.occ = occ;
+  c->gtune.ord = ord;
+  c->gtune.bx = bx;
+  c->gtune.stages = stages;
+  c->gtune.cpc = cpc;
+  return 0;
+}
+
+int wlg_gram_shape(wlg_ctx* c, int msl, int mwlt, int* shape) {
+  CTX_BEGIN(c);
+  GramPlan gp;
+  if (!shape || !gram_plan(gp, c->g, c->bc, msl, mwlt, c->prec == WLG_FP64, &c->gtune)) {
+    set_error("no temporal-gauge plan for msl %d, mwlt %d", msl, mwlt);
+    return -1;
+  }
+  const int v[10] = {gp.TQ, gp.occ, gp.ord + 1, gp.BX, gp.nblk, gp.stages, gp.cpc, gp.nsplit,
+                     gp.block, (int)(gp.smem / 1024)};
+  for (int i = 0; i < 10; i++) shape[i] = v[i];
+  return 0;
+}
 
 int wlg_contract_form(wlg_ctx* c, int* form) {
   CTX_BEGIN(c);

@@ -310,10 +310,9 @@ __global__ void __launch_bounds__(128) k_gauge_line_step(Geo g, int Nu, int ntil
 // thread's swizzle is fixed.  Thread (i, gq) owns start slice x0 = blk*BX + i
 // and the TQ extents T = gq + 1 + NG j (j < TQ): per 16-byte column group it
 // reads the L A-vectors of its slice and, one at a time, the L B-vectors of
-// each partner slice, advancing the L sums of a B vector one component at a
-// time (L independent FMAs between two updates of one sum).  At most 192
-// threads and 170 registers a thread, so two blocks share an SM and one
-// computes while the other waits at its barrier.  Lanes of a warp share start slices
+// each partner slice, and advances the L sums of a B vector (the order of
+// the FMAs and the occupancy -- one block of 256 or two of 192 threads per
+// SM -- are kernel variants; the plan picks one per precision).  Lanes of a warp share start slices
 // (broadcast reads), and the partner rows one read of a warp touches span at
 // most 32/NG + NG - 1 consecutive slices.
 // ---------------------------------------------------------------------------
@@ -347,7 +346,10 @@ __device__ __forceinline__ void gcp_wait(int n) {
 }
 
 constexpr int kRowBytes = 128;
-constexpr int kMaxGramThreads = 192;  // two blocks per SM: at most 170 registers a thread
+// occupancy variants: OCC 1 = one block of up to 256 threads per SM (255
+// registers a thread), OCC 2 = two blocks of up to 192 threads (170 registers)
+__host__ __device__ constexpr int gram_threads(int occ) { return occ == 2 ? 192 : 256; }
+constexpr int kMaxGramThreads = 256;
 constexpr unsigned kNoRow = 0xffffffffu;
 
 struct GramArgs {
@@ -361,8 +363,11 @@ struct GramArgs {
 __host__ __device__ __forceinline__ int gram_tab_bytes(int nrows) { return (nrows * 4 + 127) & ~127; }
 __host__ __device__ __forceinline__ int round8(int v) { return (v + 7) & ~7; }
 
-template <class E, int L, int TQ>
-__global__ void __launch_bounds__(kMaxGramThreads, 2) k_gram(GramArgs P) {
+// ORD 0: each B vector's dot products as chains of VN dependent FMAs (the L
+// chains of one B vector interleave); ORD 1: one component at a time over
+// the L sums of a B vector
+template <class E, int L, int TQ, int OCC, int ORD>
+__global__ void __launch_bounds__(gram_threads(OCC), OCC) k_gram(GramArgs P) {
   constexpr int KW = 128 / (int)sizeof(E);
   constexpr int VN = GVec<E>::N;
   typedef typename GVec<E>::t V;
@@ -457,11 +462,19 @@ __global__ void __launch_bounds__(kMaxGramThreads, 2) k_gram(GramArgs P) {
 #pragma unroll
         for (int s2 = 0; s2 < L; s2++) {
           const V b = *reinterpret_cast<const V*>(bp + s2 * bstride);
-#pragma unroll
-          for (int c = 0; c < VN; c++)
+          if constexpr (ORD == 0) {
 #pragma unroll
             for (int s1 = 0; s1 < L; s1++)
-              acc[j][s1][s2] = fma(comp(a[s1], c), comp(b, c), acc[j][s1][s2]);
+#pragma unroll
+              for (int c = 0; c < VN; c++)
+                acc[j][s1][s2] = fma(comp(a[s1], c), comp(b, c), acc[j][s1][s2]);
+          } else {
+#pragma unroll
+            for (int c = 0; c < VN; c++)
+#pragma unroll
+              for (int s1 = 0; s1 < L; s1++)
+                acc[j][s1][s2] = fma(comp(a[s1], c), comp(b, c), acc[j][s1][s2]);
+          }
         }
       }
     }
@@ -506,39 +519,50 @@ __global__ void __launch_bounds__(256) k_gram_reduce(const E* __restrict__ parti
 }
 
 // ---------------------------------------------------------------------------
-// Instantiations: (levels L, extents per thread TQ).  FP32 keeps at most
-// 128 sums per thread, FP64 at most 64 (128 registers), within 170.
+// Instantiations (element, levels L, extents per thread TQ, occupancy OCC,
+// FMA order ORD).  The first entry of a (type, L) pair is its default; the
+// others are tuning candidates.  FP32 keeps at most 128 sums per thread,
+// FP64 at most 64 doubles in OCC 2 (170 registers) and 72 in OCC 1.
 // ---------------------------------------------------------------------------
-#define WLG_GRAM_F32(X) X(float, 1, 8) X(float, 2, 8) X(float, 3, 6) X(float, 4, 6) \
-  X(float, 4, 4) X(float, 5, 4) X(float, 6, 3) X(float, 6, 2) X(float, 7, 2) X(float, 8, 2)
-#define WLG_GRAM_F64(X) X(double, 1, 8) X(double, 2, 6) X(double, 3, 4) X(double, 4, 3) \
-  X(double, 4, 2) X(double, 5, 2) X(double, 6, 1) X(double, 7, 1) X(double, 8, 1)
+#define WLG_GRAM_VARIANTS(X)                                                                   \
+  X(float, 1, 8, 1, 0) X(float, 2, 8, 1, 0) X(float, 3, 6, 1, 0) X(float, 4, 6, 1, 0)           \
+  X(float, 4, 4, 1, 0) X(float, 5, 4, 1, 0) X(float, 6, 3, 1, 0) X(float, 6, 3, 1, 1)           \
+  X(float, 6, 3, 2, 0) X(float, 6, 3, 2, 1) X(float, 7, 2, 1, 0) X(float, 8, 2, 1, 0)           \
+  X(double, 1, 8, 2, 1) X(double, 2, 6, 2, 1) X(double, 3, 4, 2, 1) X(double, 4, 3, 2, 1)       \
+  X(double, 4, 2, 2, 1) X(double, 5, 2, 2, 1) X(double, 6, 1, 2, 1) X(double, 6, 1, 2, 0)       \
+  X(double, 6, 2, 1, 0) X(double, 6, 2, 1, 1) X(double, 7, 1, 2, 1) X(double, 8, 1, 2, 1)
 
-template <class E> struct GramKernel {
-  static void* get(int L, int TQ) {
-#define WLG_GRAM_PICK(ET, LL, TT) \
-  if (sizeof(E) == sizeof(ET) && L == LL && TQ == TT) return (void*)k_gram<ET, LL, TT>;
-    WLG_GRAM_F32(WLG_GRAM_PICK)
-    WLG_GRAM_F64(WLG_GRAM_PICK)
+void* gram_kernel(int esize, int L, int TQ, int occ, int ord) {
+#define WLG_GRAM_PICK(ET, LL, TT, OO, RR)                                                     \
+  if (esize == (int)sizeof(ET) && L == LL && TQ == TT && occ == OO && ord == RR)              \
+    return (void*)k_gram<ET, LL, TT, OO, RR>;
+  WLG_GRAM_VARIANTS(WLG_GRAM_PICK)
 #undef WLG_GRAM_PICK
-    return nullptr;
-  }
-};
+  return nullptr;
+}
 
-// candidate extents per thread for L levels, best first
-template <class E> static void tq_candidates(int L, int out[2]) {
-  out[0] = out[1] = 0;
+struct GramVariant {
+  int TQ, occ, ord;
+};
+// the variants for (esize, L) that match the requested occupancy / order
+// (0: any), in table order
+static int gram_variants(int esize, int L, int occ, int ord, GramVariant* out, int max) {
   int n = 0;
-#define WLG_GRAM_TQ(ET, LL, TT) \
-  if (sizeof(E) == sizeof(ET) && L == LL && n < 2) out[n++] = TT;
-  WLG_GRAM_F32(WLG_GRAM_TQ)
-  WLG_GRAM_F64(WLG_GRAM_TQ)
-#undef WLG_GRAM_TQ
+#define WLG_GRAM_LIST(ET, LL, TT, OO, RR)                                                     \
+  if (esize == (int)sizeof(ET) && L == LL && (occ == 0 || occ == OO) &&                      \
+      (ord == 0 || ord - 1 == RR) && n < max)                                                 \
+    out[n++] = GramVariant{TT, OO, RR};
+  WLG_GRAM_VARIANTS(WLG_GRAM_LIST)
+#undef WLG_GRAM_LIST
+  return n;
 }
 
 }  // namespace
 
-bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64) {
+bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64,
+               const GramTuning* tune) {
+  GramTuning none;
+  if (!tune) tune = &none;
   p = GramPlan();
   if (msl < 1 || msl > 8 || mwlt < 1) return false;
   const int esz = fp64 ? 8 : 4;
@@ -548,48 +572,47 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64) 
   p.ntile = (g.vs + 31) / 32;
   p.A = (size_t)p.Nu * p.ntile * kSlabTile;
   p.Aa = (size_t)g.n[0] * p.ntile * kSlabTile;
-  int cand[2];
-  if (fp64)
-    tq_candidates<double>(msl, cand);
-  else
-    tq_candidates<float>(msl, cand);
-  // extents per thread: the candidate that wastes the fewest (ties: the first)
+  GramVariant cand[16];
+  const int nc = gram_variants(esz, msl, tune->occ, tune->ord, cand, 16);
+  // the default variant of the level count's first occupancy and order, with
+  // the extents per thread that waste the fewest (ties: the first listed)
   int best = -1, bw = 1 << 30;
-  for (int c = 0; c < 2; c++) {
-    if (cand[c] <= 0) continue;
-    const int ng = (mwlt + cand[c] - 1) / cand[c];
-    const int waste = ng * cand[c] - mwlt;
+  for (int c = 0; c < nc; c++) {
+    if (cand[c].occ != cand[0].occ || cand[c].ord != cand[0].ord) continue;
+    const int ng = (mwlt + cand[c].TQ - 1) / cand[c].TQ;
+    const int waste = ng * cand[c].TQ - mwlt;
     if (waste < bw) {
       bw = waste;
-      best = cand[c];
+      best = c;
     }
   }
-  if (best <= 0) return false;
-  p.TQ = best;
-  p.NG = (mwlt + best - 1) / best;
-  if (p.NG > kMaxGramThreads) return false;
+  if (best < 0) return false;
+  p.TQ = cand[best].TQ;
+  p.occ = cand[best].occ;
+  p.ord = cand[best].ord;
+  p.NG = (mwlt + p.TQ - 1) / p.TQ;
+  const int cap = gram_threads(p.occ);
+  if (p.NG > cap) return false;
   const int N0 = g.n[0];
-  const int bxmax = kMaxGramThreads / p.NG;
-  // the fewest start-slice blocks whose rows fit two stages in half an SM's
-  // shared memory (two blocks per SM), else in a whole SM's
-  const size_t smem_half = 113 * 1024, smem_max = 227 * 1024;
-  for (int pass = 0; pass < 2 && p.BX == 0; pass++) {
-    const size_t lim = pass == 0 ? smem_half : smem_max;
-    for (int nblk = (N0 + bxmax - 1) / bxmax; nblk <= N0; nblk++) {
-      const int BX = (N0 + nblk - 1) / nblk;
-      const int nrows = msl * (round8(BX) + round8(BX + mwlt - 1));
-      const size_t tab = (size_t)gram_tab_bytes(nrows), per = (size_t)nrows * kRowBytes;
-      if (tab + 2 * per > lim) continue;
-      p.BX = BX;
-      p.BXp = round8(BX);
-      p.nblk = (N0 + BX - 1) / BX;
-      p.NYB = BX + mwlt - 1;
-      p.NYBp = round8(p.NYB);
-      p.nrows = nrows;
-      p.stages = (int)std::min<size_t>(4, (lim - tab) / per);
-      p.smem = tab + (size_t)p.stages * per;
-      break;
-    }
+  const int bxmax = std::min(cap / p.NG, tune->bx > 0 ? tune->bx : N0);
+  // the fewest start-slice blocks whose rows fit two stages in the shared
+  // memory of one block (half an SM's for two blocks per SM)
+  const size_t lim = p.occ == 2 ? 113 * 1024 : 227 * 1024;
+  for (int nblk = (N0 + bxmax - 1) / bxmax; nblk <= N0; nblk++) {
+    const int BX = (N0 + nblk - 1) / nblk;
+    const int nrows = msl * (round8(BX) + round8(BX + mwlt - 1));
+    const size_t tab = (size_t)gram_tab_bytes(nrows), per = (size_t)nrows * kRowBytes;
+    if (tab + 2 * per > lim) continue;
+    p.BX = BX;
+    p.BXp = round8(BX);
+    p.nblk = (N0 + BX - 1) / BX;
+    p.NYB = BX + mwlt - 1;
+    p.NYBp = round8(p.NYB);
+    p.nrows = nrows;
+    p.stages = (int)std::min<size_t>(4, (lim - tab) / per);
+    if (tune->stages >= 2 && tune->stages < p.stages) p.stages = tune->stages;
+    p.smem = tab + (size_t)p.stages * per;
+    break;
   }
   if (p.BX == 0) return false;
   // row offsets are kept as 32-bit multiples of 16 bytes
@@ -611,6 +634,7 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64) 
     const long long acc_cap = (long long)std::sqrt((double)p.nchunks / 32.0);
     cpc = std::max(1LL, std::min(cpc, acc_cap));
   }
+  if (tune->cpc > 0) cpc = tune->cpc;
   p.cpc = (int)cpc;
   p.nsplit = (p.nchunks + p.cpc - 1) / p.cpc;
   p.partial_elems = (size_t)p.nsplit * N0 * mwlt * msl * msl;
@@ -673,17 +697,12 @@ void gram_contract(const Geo& g, const GramPlan& p, int mwlt, const T* alines, c
   a.cpc = p.cpc;
   a.stages = p.stages;
   a.nrows = p.nrows;
-  void* fn = GramKernel<T>::get(p.L, p.TQ);
+  void* fn = gram_kernel((int)sizeof(T), p.L, p.TQ, p.occ, p.ord);
   if (!fn) {
     set_error("kernel gram: none for %d levels and %d extents per thread", p.L, p.TQ);
     return;
   }
-  static bool attr[2][9][9];
-  bool& done = attr[sizeof(T) == 8][p.L][p.TQ];
-  if (!done) {
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    done = true;
-  }
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   void* args[] = {&a};
   cudaLaunchKernel(fn, dim3(p.nblk * p.nsplit), dim3(p.block), args, p.smem, st);
   WLG_LAUNCH_CHECK("gram");

@@ -131,13 +131,21 @@ struct GramPlan {
   int ntile = 0;    // 32-site tiles per time slice
   size_t A = 0;     // elements of one slab array over Nu slices
   size_t Aa = 0;    // elements of one slab array over N0 slices (the A lines)
-  int TQ = 0, NG = 0, BX = 0, BXp = 0, NYB = 0, NYBp = 0, nblk = 0, nrows = 0, stages = 0;
+  int TQ = 0, occ = 0, ord = 0;  // kernel variant: extents per thread, blocks per SM, FMA order
+  int NG = 0, BX = 0, BXp = 0, NYB = 0, NYBp = 0, nblk = 0, nrows = 0, stages = 0;
   int block = 0;
   size_t smem = 0;  // dynamic shared memory per block
   int nchunks = 0, cpc = 0, nsplit = 0;
   size_t partial_elems = 0;
 };
-bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64);
+// Tuning of the Gram stage (0: automatic): blocks per SM (1, 2), FMA order
+// (1: dot-product chains, 2: component-major), start slices per block (an
+// upper bound), pipeline stages, column chunks per block.
+struct GramTuning {
+  int occ = 0, ord = 0, bx = 0, stages = 0, cpc = 0;
+};
+bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64,
+               const GramTuning* tune = nullptr);
 // The gauge field g and H^-1 = (g g^dag)^-1 (FP64 slabs of A doubles each)
 // from the temporal links u0; *dev (device) receives max |g g^dag - 1| as the
 // bits of a non-negative double (the form is not used when it exceeds 1/4).
