@@ -1,6 +1,7 @@
-"""Contraction forms that tests pin when they compare a single context with
-the batch path bit for bit: the batch path runs the carried-temporal-line
-forms (10 mixed, 7 FP64), a context the temporal-gauge form by default."""
+"""The carried-temporal-line contraction form a context runs when the
+temporal-gauge form is switched off (10 mixed, 7 FP64; also the form of
+lattices smeared without projection); tests pin it to compare the
+carried-line shapes with each other, or the two forms with each other."""
 
 
 def carried_form(prec: str) -> int:

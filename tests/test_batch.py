@@ -8,7 +8,6 @@ import pytest
 
 from tests import oracle as O
 from wloop_b200 import APE, HYP, Context, WloopParms, generate_links
-from tests.forms import carried_form
 from wloop_b200.api import Batch
 from wloop_b200.autotune import candidates
 from wloop_b200.workloads import batch_workloads, flops_per_config
@@ -40,10 +39,10 @@ def test_autotune_candidates():
     assert all(G <= 4 for G, _, _, _ in candidates(4, False, True))
     assert (6, 1, 64, 0) in candidates(6, False, False)
     assert all(G <= 3 and b == 64 for G, SB, b, _ in candidates(6, True, False) if SB != 11)
-    # the temporal-gauge form (SB 11) is a context candidate, first, and no batch one
+    # the temporal-gauge form (SB 11) is the first candidate of contexts and batches
     for fp64 in (False, True):
-        assert candidates(6, fp64, False)[0] == (0, 11, 0, 0)
-        assert not any(SB == 11 for _, SB, _, _ in candidates(6, fp64, True))
+        for batched in (False, True):
+            assert candidates(6, fp64, batched)[0] == (0, 11, 0, 0)
     # packed-FMA batch shapes (SB 5) for FP32 batches with unrolled level counts only
     assert any(SB == 5 for _, SB, _, _ in candidates(6, False, True))
     assert not any(SB == 5 for _, SB, _, _ in candidates(6, True, True))
@@ -57,7 +56,6 @@ def test_batch_equals_single_contexts(prec):
     singles = []
     for (n, bc, p), u in zip(ITEMS, fields):
         with Context(n, bc, prec) as c:
-            c.set_contract_tuning(variant=carried_form(prec))
             c.upload(u)
             singles.append(c.measure(p))
     with Batch(ITEMS, prec) as b:
@@ -77,7 +75,6 @@ def test_batch_equals_single_contexts(prec):
         b.upload(1, u2)
         b.run()
         with Context(ITEMS[1][0], ITEMS[1][1], prec) as c:
-            c.set_contract_tuning(variant=carried_form(prec))
             c.upload(u2)
             ref1 = c.measure(ITEMS[1][2])
         assert np.array_equal(b.result(1), ref1)
@@ -120,7 +117,6 @@ def test_batch_generate_and_shape_change():
             scale = np.maximum(np.abs(r0[i]), 1e-3)
             assert np.max(np.abs(b.result(i) - r0[i]) / scale) < 1e-6
         with Context(items[0][0], items[0][1], "mixed") as c:
-            c.set_contract_tuning(variant=carried_form("mixed"))
             c.generate(7, 0.2)
             assert np.array_equal(c.measure(items[0][2]), r0[0])
 

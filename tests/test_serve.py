@@ -12,7 +12,6 @@ import numpy as np
 import pytest
 
 from wloop_b200 import APE, Context, WloopParms, generate_links
-from tests.forms import carried_form
 from wloop_b200.api import Server, estimate_bytes
 
 P = WloopParms(msl=3, nss=[0, 2, 2], mwlt=3, mwlr=2, op_smear=APE, alpha_ape=0.5, proj_iter=4)
@@ -50,7 +49,6 @@ def test_result_same_alone_and_in_mix():
     # every result equals a plain context measurement of the same field
     for o, (res, _, _) in zip(others, outs):
         with Context(o[0], o[1], "mixed") as c:
-            c.set_contract_tuning(variant=carried_form("mixed"))
             c.generate(o[2], o[3])
             assert np.array_equal(c.measure(P), res)
 
@@ -62,7 +60,6 @@ def test_host_field_request_matches_context():
     with Server(max_inflight=1) as s:
         res, _, _ = s.wait(s.submit(n, bc, P, "fp64", links=u))
     with Context(n, bc, "fp64") as c:
-        c.set_contract_tuning(variant=carried_form("fp64"))
         c.upload(u)
         assert np.array_equal(c.measure(P), res)
 
@@ -157,6 +154,5 @@ def test_mixed_lattices_share_a_batch_and_match_alone():
     assert max(bs for _, _, bs in outs) > 1
     for (n, bc, p, sd), (res, _, _) in zip(reqs, outs):
         with Context(n, bc, "mixed") as c:
-            c.set_contract_tuning(variant=carried_form("mixed"))
             c.generate(sd, 0.3)
             assert np.array_equal(c.measure(p), res)

@@ -73,10 +73,9 @@ def candidates(msl: int, fp64: bool, batched: bool) -> List[Shape]:
         # the ninth form (one 32-column chunk per warp, four blocks per SM),
         # marked SB 9; single contexts only, with its own G and block
         out.append(((msl + 1) // 2, 9, 128, 0))
-    if not batched:
-        # the temporal-gauge form (banded Gram product), marked SB 11; it
-        # plans its own shapes
-        out.insert(0, (0, 11, 0, 0))
+    # the temporal-gauge form (banded Gram product), marked SB 11; it plans
+    # its own shapes (a batch runs it for the lattices whose smearing projects)
+    out.insert(0, (0, 11, 0, 0))
     return out
 
 
@@ -176,4 +175,6 @@ def _form(G: int, SB: int, fp64: bool) -> int:
 
 def _as_batch(shape: Shape):
     G, SB, block, nCB = shape
+    if SB == 11:
+        return 0, 0, 0, 0  # the default plan: the temporal-gauge form where it applies
     return G, SB, nCB, block

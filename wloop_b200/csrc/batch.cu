@@ -11,6 +11,13 @@
 // has finished for every lattice before the first sweep writes there).  The
 // contraction forms 4-7 write the next R's lines themselves, alternating
 // between the two line buffers; the third form runs a line-step stage.
+// Configurations whose smearing projects (proj_iter >= 3) run the
+// temporal-gauge form (gram.cu) instead, one launch per lattice and stage
+// inside the same graph: its g and H^-1 take the APE ping-pong slots, its A
+// lines the level store (dead once the first lines exist), its recursion
+// links and B lines start at the first line buffer, the region grown where
+// they need more; the carried-line shapes of wlg_batch_set_contract_shape
+// switch it off.  A run fails if g g^dag of such a lattice is far from 1.
 #include <string.h>
 
 #include <algorithm>
@@ -34,9 +41,14 @@ struct Cfg {
   size_t partial;            // byte offset in the partial-sum buffer
   size_t nwl;
   size_t wl_host;  // offset (doubles) in the pinned result block
+  // temporal-gauge form: eligible (layout) and in use (plan), its plan and
+  // the byte offsets of its buffers in the arena
+  bool gram_ok, gram;
+  GramPlan gp;
+  size_t gG, gH, gUh, gB, gA, gDev;
 };
 
-enum OpKind { OP_SMEAR, OP_COPY, OP_LINES, OP_CONTRACT, OP_REDUCE, OP_D2H };
+enum OpKind { OP_SMEAR, OP_COPY, OP_LINES, OP_CONTRACT, OP_REDUCE, OP_D2H, OP_GRAM_PREP, OP_GRAM_R };
 
 struct Op {
   int kind;
@@ -50,6 +62,7 @@ struct Op {
   void* dst;
   const void* src;
   size_t bytes;
+  int cfg, R;  // OP_GRAM_PREP / OP_GRAM_R: the lattice and the spatial extent
 };
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -67,6 +80,7 @@ struct wlg_batch {
   char* tables = nullptr;
   double* wl_host = nullptr;  // pinned
   size_t wl_host_doubles = 0;
+  unsigned long long* dev_host = nullptr;  // pinned: |g g^dag - 1| per lattice (bits)
   char* staging = nullptr;    // device AoS staging for uploads
   size_t staging_bytes = 0;
   std::vector<Op> ops;
@@ -310,6 +324,24 @@ template <class T> void build_ops(wlg_batch* b) {
   }
 
   // ---- loops (wloop.c:524-608) ----
+  // temporal-gauge lattices: g, H^-1 and the first lines, then per R their
+  // line step, Gram product and reduction (one launch per lattice)
+  for (int c = 0; c < n; c++) {
+    if (!b->cfg[c].gram) continue;
+    Op op{};
+    op.kind = OP_GRAM_PREP;
+    op.cfg = c;
+    b->ops.push_back(op);
+  }
+  for (int r = 0; r < maxr; r++)
+    for (int c = 0; c < n; c++) {
+      if (!b->cfg[c].gram || r >= b->cfg[c].p.mwlr) continue;
+      Op op{};
+      op.kind = OP_GRAM_R;
+      op.cfg = c;
+      op.R = r + 1;
+      b->ops.push_back(op);
+    }
   for (int r = 0; r < maxr; r++) {
     const int R = r + 1;
     std::vector<LArgs<T>> la;
@@ -325,7 +357,7 @@ template <class T> void build_ops(wlg_batch* b) {
     std::vector<Group> groups;
     for (int c = 0; c < n; c++) {
       const Cfg& f = b->cfg[c];
-      if (r >= f.p.mwlr) continue;
+      if (r >= f.p.mwlr || f.gram) continue;
       const T2* lev = (const T2*)levels[c];
       const T2* L = lev;
       const bool fuse = contract_fuses_lines(f.cp);
@@ -413,6 +445,12 @@ template <class T> void build_ops(wlg_batch* b) {
     op.src = base(f.wl);
     op.bytes = f.nwl * sizeof(double);
     b->ops.push_back(op);
+    if (f.gram) {
+      op.dst = b->dev_host + c;
+      op.src = base(f.gDev);
+      op.bytes = sizeof(unsigned long long);
+      b->ops.push_back(op);
+    }
   }
   b->host_tables.swap(tb.bytes);
 }
@@ -448,6 +486,39 @@ template <class T> int issue(wlg_batch* b) {
       case OP_D2H:
         WLG_CUDA(cudaMemcpyAsync(op.dst, op.src, op.bytes, cudaMemcpyDeviceToHost, b->st));
         break;
+      case OP_GRAM_PREP: {
+        const Cfg& f = b->cfg[op.cfg];
+        typedef typename V2<T>::t T2;
+        char* r = b->arena + f.region;
+        const size_t es = elem_bytes(b);
+        gauge_chain<T>(f.g, f.gp, lview<T>(b->arena + f.U, f.D, 4, 0).p[0],
+                       (double*)(b->arena + f.gG), (double*)(b->arena + f.gH),
+                       (unsigned long long*)(b->arena + f.gDev), b->st);
+        gauge_first<T>(f.g, f.gp, f.p.msl, (const T2*)(r + 6 * f.D * es),
+                       (const double*)(b->arena + f.gG), (const double*)(b->arena + f.gH),
+                       (T*)(b->arena + f.gUh), (T*)(b->arena + f.gB), nullptr, b->st);
+        // the A lines of length 1 (they may overwrite the level store)
+        gram_line_step<T>(f.g, f.gp, f.p.msl, 1, (const T*)(b->arena + f.gUh),
+                          (const double*)(b->arena + f.gH), (T*)(b->arena + f.gB),
+                          (T*)(b->arena + f.gA), b->st);
+        kernels += 3;
+        break;
+      }
+      case OP_GRAM_R: {
+        const Cfg& f = b->cfg[op.cfg];
+        T* bl = (T*)(b->arena + f.gB);
+        T* al = (T*)(b->arena + f.gA);
+        if (op.R >= 2) {
+          gram_line_step<T>(f.g, f.gp, f.p.msl, op.R, (const T*)(b->arena + f.gUh),
+                            (const double*)(b->arena + f.gH), bl, al, b->st);
+          kernels++;
+        }
+        gram_contract<T>(f.g, f.gp, f.p.mwlt, al, bl, (T*)(b->pbuf + f.partial), b->st);
+        gram_reduce<T>(f.g, f.gp, f.bc, f.p.mwlt, f.p.mwlr, op.R - 1,
+                       (const T*)(b->pbuf + f.partial), (double*)(b->arena + f.wl), b->st);
+        kernels += 2;
+        break;
+      }
     }
   }
   b->kernels = kernels;
@@ -472,6 +543,12 @@ int plan(wlg_batch* b) {
     if (f.cp.SB == 5 && fp64) f.cp.SB = 3;
     f.cp.variant = (f.cp.SB == 1 || f.cp.SB == 2) ? 3
                  : (f.cp.SB == 3 ? 5 : (f.cp.SB == 4 ? 7 : (f.cp.SB == 5 ? 10 : 4)));
+    f.gram = f.gram_ok && b->tG == 0;
+    if (f.gram) {
+      f.partial = poff;
+      poff = align256(poff + f.gp.partial_elems * (fp64 ? 8 : 4));
+      continue;
+    }
     if (f.cp.G > 4) {
       set_error("batch: contraction shape G=%d is not available in batched form", f.cp.G);
       return -1;
@@ -498,7 +575,43 @@ void layout(wlg_batch* b) {
     // APE ping-pong 6 + levels 3 msl + lines 3 msl + spatial-HYP scratch 6 +
     // second lines 3 msl, or the HYP scratch (24), whichever is larger
     size_t rdirs = std::max<size_t>(24, 12 + 9 * (size_t)f.p.msl);
-    off = align256(off + rdirs * f.D * es);
+    size_t rbytes = rdirs * f.D * es;
+    f.gram_ok = f.p.proj_iter >= 3 &&
+                gram_plan(f.gp, f.g, f.bc, f.p.msl, f.p.mwlt, fp64);
+    if (f.gram_ok) {
+      // after the smearing: g and H^-1 in the APE ping-pong slots (6 D),
+      // Uh, B and A lines from the first line buffer on
+      const size_t esz = fp64 ? 8 : 4, nb = 3 * (size_t)f.p.msl * f.gp.A * esz;
+      const size_t gh = align256(f.gp.A * sizeof(double));
+      const size_t lines_at = (6 + 3 * (size_t)f.p.msl) * f.D * es;
+      size_t o = align256(lines_at);
+      f.gUh = f.region + o;
+      o = align256(o + nb);
+      f.gB = f.region + o;
+      o = align256(o + nb);
+      // the A lines take the level store, dead once the first lines exist,
+      // where they fit in it (they are written after it is read)
+      const size_t na = 3 * (size_t)f.p.msl * f.gp.Aa * esz;
+      if (na <= 3 * (size_t)f.p.msl * f.D * es) {
+        f.gA = f.region + 6 * f.D * es;
+      } else {
+        f.gA = f.region + o;
+        o = align256(o + na);
+      }
+      f.gDev = f.region + o;
+      o = align256(o + 8);
+      if (2 * gh <= 6 * f.D * es) {
+        f.gG = f.region;
+        f.gH = f.region + gh;
+      } else {
+        f.gG = f.region + o;
+        o = align256(o + gh);
+        f.gH = f.region + o;
+        o = align256(o + gh);
+      }
+      rbytes = std::max(rbytes, o);
+    }
+    off = align256(off + rbytes);
     f.nwl = (size_t)f.p.msl * f.p.msl * f.p.mwlt * f.p.mwlr * f.g.n[0];
     f.wl = off;
     off = align256(off + f.nwl * sizeof(double));
@@ -552,6 +665,8 @@ int ensure_pbuf(wlg_batch* b) {
 
 int build(wlg_batch* b) {
   if (b->built) return 0;
+  for (const Cfg& f : b->cfg)
+    if (f.gram && gram_prepare(f.gp)) return -1;
   if (b->prec == WLG_FP64)
     build_ops<double>(b);
   else
@@ -643,7 +758,8 @@ int wlg_batch_create(int nconf, const int* dims, const int* bcs, const wlg_wloop
   }
   if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess || ensure_pbuf(b) ||
       pool_alloc(b, &b->arena, b->arena_bytes) || pool_alloc(b, &b->staging, b->staging_bytes) ||
-      cudaMallocHost(&b->wl_host, b->wl_host_doubles * sizeof(double)) != cudaSuccess) {
+      cudaMallocHost(&b->wl_host, b->wl_host_doubles * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&b->dev_host, nconf * sizeof(unsigned long long)) != cudaSuccess) {
     set_error("batch_create: cannot allocate %.2f GB arena: %s", b->arena_bytes / 1e9,
               cudaGetErrorString(cudaGetLastError()));
     wlg_batch_destroy(b);
@@ -670,6 +786,7 @@ int wlg_batch_destroy(wlg_batch* b) {
     cudaStreamSynchronize(b->st);  // the frees are ordered on the stream
   }
   if (b->wl_host) cudaFreeHost(b->wl_host);
+  if (b->dev_host) cudaFreeHost(b->dev_host);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->st) cudaStreamDestroy(b->st);
@@ -791,8 +908,19 @@ int wlg_batch_run(wlg_batch* b) {
     set_error("batch_run: %s", cudaGetErrorString(e));
     return -1;
   }
+  for (size_t c = 0; c < b->cfg.size(); c++) {
+    if (!b->cfg[c].gram) continue;
+    double dev;
+    memcpy(&dev, b->dev_host + c, sizeof(dev));
+    if (!(dev <= 0.25)) {
+      set_error("batch_run: configuration %zu: |g g^dag - 1| = %g along time, the temporal-gauge "
+                "form does not apply (a carried-line shape, wlg_batch_set_contract_shape, "
+                "measures it)", c, dev);
+      return -1;
+    }
+  }
   bool bulk = false;
-  for (const Cfg& f : b->cfg) bulk = bulk || f.cp.variant == 7;
+  for (const Cfg& f : b->cfg) bulk = bulk || (!f.gram && f.cp.variant == 7);
   if (bulk && contract_stage_failed() != 0) {
     set_error("batch_run: the contraction's staged-line copies did not arrive in time");
     return -1;

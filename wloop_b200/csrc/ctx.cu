@@ -388,7 +388,11 @@ static int do_loops_gram(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
   const Geo& g = c->g;
   const int msl = p->msl;
   GramPlan gp;
+  // the form needs projected smearing (the projection keeps the temporal
+  // links near SU(3), so g stays well conditioned)
+  if (p->proj_iter < 3) return 1;
   if (!gram_plan(gp, g, c->bc, msl, p->mwlt, c->prec == WLG_FP64, &c->gtune)) return 1;
+  if (gram_prepare(gp)) return -1;
   const size_t nb = gp.A * sizeof(T) * 3 * msl, na = gp.Aa * sizeof(T) * 3 * msl;
   const size_t nwl = (size_t)msl * msl * p->mwlt * p->mwlr * g.n[0];
   if (ensure(c->gG, gp.A * sizeof(double)) || ensure(c->gH, gp.A * sizeof(double)) ||

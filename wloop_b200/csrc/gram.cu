@@ -184,7 +184,9 @@ __global__ void __launch_bounds__(128) k_gauge_chain(Geo g, int Nu, int ntile,
 // levels per item:
 //     B1 = g(y) U_k(y mod N0) g(y+k)^dag      -> B lines   (all Nu slices)
 //     Uh = H^-1(y) B1                        -> recursion (all Nu slices)
-//     A1 = Uh H^-1(y+k)                      -> A lines   (y0 < N0)
+//     A1 = Uh H^-1(y+k)                      -> A lines   (y0 < N0; unless
+//                                           alines is null, when a line step
+//                                           with R = 1 writes them)
 // FP64 products, stored as E.
 // ---------------------------------------------------------------------------
 template <class T, class E>
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(128) k_gauge_first(Geo g, int Nu, int ntile, i
       for (int sl = 0; sl < msl; sl++) {
         zero_slab(uh + (size_t)(sl * 3 + k) * A, tile, lane);
         zero_slab(blines + (size_t)(sl * 3 + k) * A, tile, lane);
-        if (start) zero_slab(alines + (size_t)(sl * 3 + k) * Aa, tile, lane);
+        if (start && alines) zero_slab(alines + (size_t)(sl * 3 + k) * Aa, tile, lane);
       }
       continue;
     }
@@ -237,7 +239,7 @@ __global__ void __launch_bounds__(128) k_gauge_first(Geo g, int Nu, int ntile, i
       ld_slab(f, Hinv, tile, lane);
       mul(t1, f, t2);
       st_slab(uh + q * A, tile, lane, t1);
-      if (start) {
+      if (start && alines) {
         ld_slab(f, Hinv, tr, jr & 31);
         mul(t2, t1, f);
         st_slab(alines + q * Aa, tile, lane, t2);
@@ -249,7 +251,8 @@ __global__ void __launch_bounds__(128) k_gauge_first(Geo g, int Nu, int ntile, i
 // ---------------------------------------------------------------------------
 // Line step: B(y, j) <- B(y, j) Uh(y, j + (R-1) k) in place (compute_uk_long,
 // wloop.c:207-258, multiplied at the far end), and for the start slices
-// A(y, j) = H^-1(y, j) B(y, j) H^-1(y, j + R k); FP64 products.
+// A(y, j) = H^-1(y, j) B(y, j) H^-1(y, j + R k); FP64 products.  With R = 1
+// only A, from the lines of length 1.
 // ---------------------------------------------------------------------------
 template <class E>
 __global__ void __launch_bounds__(128) k_gauge_line_step(Geo g, int Nu, int ntile, int msl, int R,
@@ -275,16 +278,24 @@ __global__ void __launch_bounds__(128) k_gauge_line_step(Geo g, int Nu, int ntil
     const int j = jt * 32 + lane;
     const size_t tile = slab_tile(y0, ntile, jt);
     const bool start = y0 < g.n[0];
-    if (j >= g.vs) continue;  // zeros since the first lines
+    if (j >= g.vs) {  // B: zeros since the first lines; A: zeros written here
+      if (R == 1 && start) zero_slab(alines + (size_t)q * Aa, tile, lane);
+      continue;
+    }
+    if (R == 1 && !start) continue;
     int x[4];
     coords(g, j, x);  // slice 0: the spatial coordinates of j
     const int n_k = g.n[k + 1];
-    const int jr = shift(g, j, x[k + 1], k + 1, (R - 1) % n_k);
     M3<double> a, b, c;
-    ld_slab(a, blines + (size_t)q * A, tile, lane);
-    ld_slab(b, uh + (size_t)q * A, slab_tile(y0, ntile, jr >> 5), jr & 31);
-    mul(c, a, b);
-    st_slab(blines + (size_t)q * A, tile, lane, c);
+    if (R >= 2) {
+      const int jr = shift(g, j, x[k + 1], k + 1, (R - 1) % n_k);
+      ld_slab(a, blines + (size_t)q * A, tile, lane);
+      ld_slab(b, uh + (size_t)q * A, slab_tile(y0, ntile, jr >> 5), jr & 31);
+      mul(c, a, b);
+      st_slab(blines + (size_t)q * A, tile, lane, c);
+    } else {
+      ld_slab(c, blines + (size_t)q * A, tile, lane);
+    }
     if (start) {
       const int je = shift(g, j, x[k + 1], k + 1, R % n_k);
       ld_slab(a, Hinv, tile, lane);
@@ -629,9 +640,9 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64,
     // FP32 sums: the rounding error of one partial grows with its run of
     // n = cpc x 32 products, and the relative error of W after the FP64
     // sum of the partials as n / sqrt(all products); a run of at most
-    // sqrt(nchunks / 32) chunks keeps it at the level of the full-size
-    // lattices, whose runs are short against their column count
-    const long long acc_cap = (long long)std::sqrt((double)p.nchunks / 32.0);
+    // 2 sqrt(nchunks / 32) chunks keeps it at one level (about 1e-7 of W on
+    // the test lattices and at 32^3x64) for small and large lattices
+    const long long acc_cap = (long long)(2.0 * std::sqrt((double)p.nchunks / 32.0));
     cpc = std::max(1LL, std::min(cpc, acc_cap));
   }
   if (tune->cpc > 0) cpc = tune->cpc;
@@ -702,10 +713,26 @@ void gram_contract(const Geo& g, const GramPlan& p, int mwlt, const T* alines, c
     set_error("kernel gram: none for %d levels and %d extents per thread", p.L, p.TQ);
     return;
   }
-  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   void* args[] = {&a};
   cudaLaunchKernel(fn, dim3(p.nblk * p.nsplit), dim3(p.block), args, p.smem, st);
   WLG_LAUNCH_CHECK("gram");
+}
+
+int gram_prepare(const GramPlan& p) {
+  void* fn = gram_kernel(p.esize, p.L, p.TQ, p.occ, p.ord);
+  if (!fn) {
+    set_error("gram: no kernel for %d levels and %d extents per thread", p.L, p.TQ);
+    return -1;
+  }
+  // the limit is per kernel, not per plan: the largest any plan may use, so
+  // that plans of other lattices keep launching
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) !=
+      cudaSuccess) {
+    set_error("gram: %zu bytes of shared memory per block: %s", p.smem,
+              cudaGetErrorString(cudaGetLastError()));
+    return -1;
+  }
+  return 0;
 }
 
 template <class T>

@@ -153,15 +153,21 @@ template <class T>
 void gauge_chain(const Geo& g, const GramPlan& p, const typename V2<T>::t* u0, double* G,
                  double* Hinv, unsigned long long* dev, cudaStream_t st);
 // The recursion links uh and the lines of length 1 (blines, alines; [msl][3]
-// slab arrays of A resp. Aa elements) from the level store.
+// slab arrays of A resp. Aa elements) from the level store; with alines
+// null the A lines are left to gram_line_step with R = 1 (so that they may
+// overwrite the level store, which this call reads).
 template <class T>
 void gauge_first(const Geo& g, const GramPlan& p, int msl, const typename V2<T>::t* levels,
                  const double* G, const double* Hinv, T* uh, T* blines, T* alines,
                  cudaStream_t st);
 // blines of length R from those of length R-1 (in place), alines of length R
+// (R = 1: alines only)
 template <class T>
 void gram_line_step(const Geo& g, const GramPlan& p, int msl, int R, const T* uh,
                     const double* Hinv, T* blines, T* alines, cudaStream_t st);
+// sets the kernel's shared-memory limit for the plan (before any launch,
+// outside stream capture); 0 or -1
+int gram_prepare(const GramPlan& p);
 // partial[nsplit][N0][mwlt][L][L] of the lines of one R
 template <class T>
 void gram_contract(const Geo& g, const GramPlan& p, int mwlt, const T* alines, const T* blines,
