@@ -178,3 +178,76 @@ def _as_batch(shape: Shape):
     if SB == 11:
         return 0, 0, 0, 0  # the default plan: the temporal-gauge form where it applies
     return G, SB, nCB, block
+
+
+# ---------------------------------------------------------------------------
+# shapes of the temporal-gauge form's Gram kernel
+# ---------------------------------------------------------------------------
+def gram_shapes(prec: str):
+    """(occ, ord, bx, stages, cpc) candidates: the kernel variants (one block
+    of 256 or two of 192 threads per SM; dot-product chains or one component
+    at a time), start slices per block and pipeline depth; cpc 0 = the plan's."""
+    bxs = (32, 22, 16) if prec == "mixed" else (0, 16, 8)
+    return [(o, r, bx, st, 0) for o in (1, 2) for r in (1, 2) for bx in bxs for st in (0, 2)]
+
+
+def gram_sweep(ctx, parms, prec: str, shapes=None, reps: int = 2):
+    """Times the Gram kernel of ctx's current field for every shape (the field
+    is restored from a snapshot before each run); yields one record per
+    distinct plan with its launch time and whether the Wilson loops equal
+    those of the first plan bit for bit."""
+    import numpy as np
+    ctx.snapshot()
+    ref, seen = None, set()
+    for (o, r, bx, st, cpc) in shapes or gram_shapes(prec):
+        ctx.set_gram_tuning(o, r, bx, st, cpc)
+        try:
+            shape = ctx.gram_shape(parms.msl, parms.mwlt)
+        except Exception:
+            continue  # no kernel of this occupancy for this precision and msl
+        key = tuple(sorted(shape.items()))
+        if key in seen:
+            continue
+        seen.add(key)
+        ctx.restore()
+        wl = ctx.measure(parms)
+        if ref is None:
+            ref = wl
+        ctx.reset_kernel_times()
+        ctx.set_profiling(True)
+        for _ in range(reps):
+            ctx.restore()
+            ctx.measure(parms)
+        cm, cn = ctx.kernel_time("contract")
+        lm, ln = ctx.kernel_time("lines")
+        ctx.set_profiling(False)
+        yield {"prec": prec, **shape, "gram_ms": cm / max(1, cn), "lines_ms": lm / max(1, ln),
+               "max_diff_vs_first": float(np.abs(wl - ref).max())}
+    ctx.set_gram_tuning()
+    ctx.restore()
+
+
+def _main():
+    import argparse
+    ap = argparse.ArgumentParser(description="shape sweeps of the contraction kernels")
+    ap.add_argument("--gram-sweep", action="store_true",
+                    help="time every Gram kernel shape on the c3 workload (32^3x64)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--cpc", default="", help="comma-separated extra chunk counts per block")
+    args = ap.parse_args()
+    if not args.gram_sweep:
+        ap.error("nothing to do (--gram-sweep)")
+    from .api import Context
+    from .workloads import C3
+    w = C3
+    shapes = gram_shapes(args.precision)
+    shapes += [(1, 1, 32 if args.precision == "mixed" else 0, 0, int(c))
+               for c in args.cpc.split(",") if c]
+    with Context(w.n, w.bc, args.precision) as c:
+        c.generate(w.seed, w.eps)
+        for rec in gram_sweep(c, w.parms, args.precision, shapes):
+            print(json.dumps(rec), flush=True)
+
+
+if __name__ == "__main__":
+    _main()

@@ -46,9 +46,13 @@ struct Cfg {
   bool gram_ok, gram;
   GramPlan gp;
   size_t gG, gH, gUh, gB, gA, gDev;
+  size_t gpartial;  // byte offset of its partial sums in the partial-sum buffer
 };
 
-enum OpKind { OP_SMEAR, OP_COPY, OP_LINES, OP_CONTRACT, OP_REDUCE, OP_D2H, OP_GRAM_PREP, OP_GRAM_R };
+enum OpKind {
+  OP_SMEAR, OP_COPY, OP_LINES, OP_CONTRACT, OP_REDUCE, OP_D2H,
+  OP_GRAM_CHAIN, OP_GRAM_PREP, OP_GRAM_R
+};
 
 struct Op {
   int kind;
@@ -62,7 +66,7 @@ struct Op {
   void* dst;
   const void* src;
   size_t bytes;
-  int cfg, R;  // OP_GRAM_PREP / OP_GRAM_R: the lattice and the spatial extent
+  int cfg, R;  // OP_GRAM_*: the lattice and the spatial extent
 };
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -77,18 +81,24 @@ struct wlg_batch {
   size_t arena_bytes = 0;
   char* pbuf = nullptr;  // contraction partial sums (depends on the contraction plan)
   size_t pbuf_bytes = 0, pbuf_cap = 0;
-  char* tables = nullptr;
   double* wl_host = nullptr;  // pinned
   size_t wl_host_doubles = 0;
   unsigned long long* dev_host = nullptr;  // pinned: |g g^dag - 1| per lattice (bits)
   char* staging = nullptr;    // device AoS staging for uploads
   size_t staging_bytes = 0;
-  std::vector<Op> ops;
-  std::vector<char> host_tables;
-  bool built = false;      // argument tables on the device
-  bool use_graph = true;   // capture the pipeline after the first run and replay it
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  // phase 0: smearing and the gauge chains; phase 1: the loops, per lattice
+  // in the form phase 0's deviations allow (use_gram)
+  struct Phase {
+    std::vector<Op> ops;
+    std::vector<char> host_tables;
+    char* tables = nullptr;
+    bool built = false;  // argument tables on the device
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;  // kernels one run of the phase launches
+  } ph[2];
+  std::vector<char> use_gram;  // per lattice: the temporal-gauge form runs in phase 1
+  bool use_graph = true;       // capture each phase after its first run and replay it
   int tG = 0, tSB = 0, tBlock = 0, tNCB = 0;  // contraction shape override (tuning)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
@@ -176,10 +186,21 @@ struct Tables {
   }
 };
 
-template <class T> void build_ops(wlg_batch* b) {
+template <class T> void build_ops(wlg_batch* b, int phase) {
   typedef typename V2<T>::t T2;
   Tables tb;
-  b->ops.clear();
+  std::vector<Op> all;  // ops are generated for both phases; this phase's are kept
+  int cur_phase = 0;    // phase of the ops generated next
+  std::vector<int> phase_of;
+  struct OpSink {
+    std::vector<Op>* v;
+    std::vector<int>* ph;
+    int* cur;
+    void push_back(const Op& o) {
+      v->push_back(o);
+      ph->push_back(*cur);
+    }
+  } sink{&all, &phase_of, &cur_phase};
   const int n = (int)b->cfg.size();
   auto base = [&](size_t off) { return b->arena + off; };
   auto push_smear = [&](int stage, const std::vector<SArgs<T>>& A, const std::vector<long long>& u) {
@@ -192,7 +213,7 @@ template <class T> void build_ops(wlg_batch* b) {
     op.n = (int)A.size();
     op.total = 0;
     for (long long x : u) op.total += x;
-    b->ops.push_back(op);
+    sink.push_back(op);
   };
   auto push_copy = [&](void* dst, const void* src, size_t bytes) {
     Op op{};
@@ -200,7 +221,7 @@ template <class T> void build_ops(wlg_batch* b) {
     op.dst = dst;
     op.src = src;
     op.bytes = bytes;
-    b->ops.push_back(op);
+    sink.push_back(op);
   };
 
   // ---- HYP (hyp_links, all directions) ----
@@ -323,24 +344,41 @@ template <class T> void build_ops(wlg_batch* b) {
     }
   }
 
-  // ---- loops (wloop.c:524-608) ----
-  // temporal-gauge lattices: g, H^-1 and the first lines, then per R their
-  // line step, Gram product and reduction (one launch per lattice)
+  // ---- phase 0 ends with the gauge chains of the temporal-gauge lattices
+  // and the read-back of their deviations from unitarity ----
   for (int c = 0; c < n; c++) {
     if (!b->cfg[c].gram) continue;
     Op op{};
+    op.kind = OP_GRAM_CHAIN;
+    op.cfg = c;
+    sink.push_back(op);
+    op.kind = OP_D2H;
+    op.dst = b->dev_host + c;
+    op.src = base(b->cfg[c].gDev);
+    op.bytes = sizeof(unsigned long long);
+    sink.push_back(op);
+  }
+  cur_phase = 1;
+  auto gram_on = [&](int c) { return c < (int)b->use_gram.size() && b->use_gram[c]; };
+
+  // ---- loops (wloop.c:524-608) ----
+  // temporal-gauge lattices: the first lines, then per R their line step,
+  // Gram product and reduction (one launch per lattice)
+  for (int c = 0; c < n; c++) {
+    if (!gram_on(c)) continue;
+    Op op{};
     op.kind = OP_GRAM_PREP;
     op.cfg = c;
-    b->ops.push_back(op);
+    sink.push_back(op);
   }
   for (int r = 0; r < maxr; r++)
     for (int c = 0; c < n; c++) {
-      if (!b->cfg[c].gram || r >= b->cfg[c].p.mwlr) continue;
+      if (!gram_on(c) || r >= b->cfg[c].p.mwlr) continue;
       Op op{};
       op.kind = OP_GRAM_R;
       op.cfg = c;
       op.R = r + 1;
-      b->ops.push_back(op);
+      sink.push_back(op);
     }
   for (int r = 0; r < maxr; r++) {
     const int R = r + 1;
@@ -357,7 +395,7 @@ template <class T> void build_ops(wlg_batch* b) {
     std::vector<Group> groups;
     for (int c = 0; c < n; c++) {
       const Cfg& f = b->cfg[c];
-      if (r >= f.p.mwlr || f.gram) continue;
+      if (r >= f.p.mwlr || gram_on(c)) continue;
       const T2* lev = (const T2*)levels[c];
       const T2* L = lev;
       const bool fuse = contract_fuses_lines(f.cp);
@@ -411,7 +449,7 @@ template <class T> void build_ops(wlg_batch* b) {
       op.pre = tb.add_prefix(lu);
       op.n = (int)la.size();
       for (long long x : lu) op.total += x;
-      b->ops.push_back(op);
+      sink.push_back(op);
     }
     for (auto& gr : groups) {
       Op op{};
@@ -425,7 +463,7 @@ template <class T> void build_ops(wlg_batch* b) {
       op.block = gr.block;
       op.msl = gr.msl;
       op.smem = gr.smem;
-      b->ops.push_back(op);
+      sink.push_back(op);
     }
     if (!ra.empty()) {
       Op op{};
@@ -434,7 +472,7 @@ template <class T> void build_ops(wlg_batch* b) {
       op.pre = tb.add_prefix(ru);
       op.n = (int)ra.size();
       for (long long x : ru) op.total += x;
-      b->ops.push_back(op);
+      sink.push_back(op);
     }
   }
   for (int c = 0; c < n; c++) {
@@ -444,56 +482,59 @@ template <class T> void build_ops(wlg_batch* b) {
     op.dst = b->wl_host + f.wl_host;
     op.src = base(f.wl);
     op.bytes = f.nwl * sizeof(double);
-    b->ops.push_back(op);
-    if (f.gram) {
-      op.dst = b->dev_host + c;
-      op.src = base(f.gDev);
-      op.bytes = sizeof(unsigned long long);
-      b->ops.push_back(op);
-    }
+    sink.push_back(op);
   }
-  b->host_tables.swap(tb.bytes);
+  b->ph[phase].ops.clear();
+  for (size_t k = 0; k < all.size(); k++)
+    if (phase_of[k] == phase) b->ph[phase].ops.push_back(all[k]);
+  b->ph[phase].host_tables.swap(tb.bytes);
 }
 
-template <class T> int issue(wlg_batch* b) {
+template <class T> int issue(wlg_batch* b, int phase) {
   int kernels = 0;
-  for (const Op& op : b->ops) {
+  const char* tables = b->ph[phase].tables;
+  for (const Op& op : b->ph[phase].ops) {
     switch (op.kind) {
       case OP_SMEAR:
-        smear_batch<T>(op.stage, (const SArgs<T>*)(b->tables + op.tab),
-                       (const long long*)(b->tables + op.pre), op.n, op.total, b->st);
+        smear_batch<T>(op.stage, (const SArgs<T>*)(tables + op.tab),
+                       (const long long*)(tables + op.pre), op.n, op.total, b->st);
         kernels++;
         break;
       case OP_COPY:
         WLG_CUDA(cudaMemcpyAsync(op.dst, op.src, op.bytes, cudaMemcpyDeviceToDevice, b->st));
         break;
       case OP_LINES:
-        line_step_batch<T>((const LArgs<T>*)(b->tables + op.tab),
-                           (const long long*)(b->tables + op.pre), op.n, op.total, b->st);
+        line_step_batch<T>((const LArgs<T>*)(tables + op.tab),
+                           (const long long*)(tables + op.pre), op.n, op.total, b->st);
         kernels++;
         break;
       case OP_CONTRACT:
-        contract_batch<T>(op.G, op.SB, (const CArgs<T>*)(b->tables + op.tab),
-                          (const long long*)(b->tables + op.pre), op.n, op.total, op.block,
+        contract_batch<T>(op.G, op.SB, (const CArgs<T>*)(tables + op.tab),
+                          (const long long*)(tables + op.pre), op.n, op.total, op.block,
                           op.smem, op.msl, b->st);
         kernels++;
         break;
       case OP_REDUCE:
-        contract_reduce_batch((const RArgs*)(b->tables + op.tab),
-                              (const long long*)(b->tables + op.pre), op.n, op.total, b->st);
+        contract_reduce_batch((const RArgs*)(tables + op.tab),
+                              (const long long*)(tables + op.pre), op.n, op.total, b->st);
         kernels++;
         break;
       case OP_D2H:
         WLG_CUDA(cudaMemcpyAsync(op.dst, op.src, op.bytes, cudaMemcpyDeviceToHost, b->st));
         break;
+      case OP_GRAM_CHAIN: {
+        const Cfg& f = b->cfg[op.cfg];
+        gauge_chain<T>(f.g, f.gp, lview<T>(b->arena + f.U, f.D, 4, 0).p[0],
+                       (double*)(b->arena + f.gG), (double*)(b->arena + f.gH),
+                       (unsigned long long*)(b->arena + f.gDev), b->st);
+        kernels++;
+        break;
+      }
       case OP_GRAM_PREP: {
         const Cfg& f = b->cfg[op.cfg];
         typedef typename V2<T>::t T2;
         char* r = b->arena + f.region;
         const size_t es = elem_bytes(b);
-        gauge_chain<T>(f.g, f.gp, lview<T>(b->arena + f.U, f.D, 4, 0).p[0],
-                       (double*)(b->arena + f.gG), (double*)(b->arena + f.gH),
-                       (unsigned long long*)(b->arena + f.gDev), b->st);
         gauge_first<T>(f.g, f.gp, f.p.msl, (const T2*)(r + 6 * f.D * es),
                        (const double*)(b->arena + f.gG), (const double*)(b->arena + f.gH),
                        (T*)(b->arena + f.gUh), (T*)(b->arena + f.gB), nullptr, b->st);
@@ -501,7 +542,7 @@ template <class T> int issue(wlg_batch* b) {
         gram_line_step<T>(f.g, f.gp, f.p.msl, 1, (const T*)(b->arena + f.gUh),
                           (const double*)(b->arena + f.gH), (T*)(b->arena + f.gB),
                           (T*)(b->arena + f.gA), b->st);
-        kernels += 3;
+        kernels += 2;
         break;
       }
       case OP_GRAM_R: {
@@ -513,16 +554,15 @@ template <class T> int issue(wlg_batch* b) {
                             (const double*)(b->arena + f.gH), bl, al, b->st);
           kernels++;
         }
-        gram_contract<T>(f.g, f.gp, f.p.mwlt, al, bl, (T*)(b->pbuf + f.partial), b->st);
+        gram_contract<T>(f.g, f.gp, f.p.mwlt, al, bl, (T*)(b->pbuf + f.gpartial), b->st);
         gram_reduce<T>(f.g, f.gp, f.bc, f.p.mwlt, f.p.mwlr, op.R - 1,
-                       (const T*)(b->pbuf + f.partial), (double*)(b->arena + f.wl), b->st);
+                       (const T*)(b->pbuf + f.gpartial), (double*)(b->arena + f.wl), b->st);
         kernels += 2;
         break;
       }
     }
   }
-  b->kernels = kernels;
-  return get_error()[0] ? -1 : 0;
+  return get_error()[0] ? -1 : kernels;
 }
 
 // contraction plans and partial-sum offsets (may change with the shape)
@@ -543,11 +583,12 @@ int plan(wlg_batch* b) {
     if (f.cp.SB == 5 && fp64) f.cp.SB = 3;
     f.cp.variant = (f.cp.SB == 1 || f.cp.SB == 2) ? 3
                  : (f.cp.SB == 3 ? 5 : (f.cp.SB == 4 ? 7 : (f.cp.SB == 5 ? 10 : 4)));
+    // the temporal-gauge form where it applies (phase 1 falls back to the
+    // carried lines per lattice, so those get their partial sums too)
     f.gram = f.gram_ok && b->tG == 0;
     if (f.gram) {
-      f.partial = poff;
+      f.gpartial = poff;
       poff = align256(poff + f.gp.partial_elems * (fp64 ? 8 : 4));
-      continue;
     }
     if (f.cp.G > 4) {
       set_error("batch: contraction shape G=%d is not available in batched form", f.cp.G);
@@ -663,50 +704,74 @@ int ensure_pbuf(wlg_batch* b) {
   return 0;
 }
 
-int build(wlg_batch* b) {
-  if (b->built) return 0;
-  for (const Cfg& f : b->cfg)
-    if (f.gram && gram_prepare(f.gp)) return -1;
+int build(wlg_batch* b, int phase) {
+  wlg_batch::Phase& P = b->ph[phase];
+  if (P.built) return 0;
+  if (phase == 1)
+    for (size_t c = 0; c < b->cfg.size(); c++)
+      if (c < b->use_gram.size() && b->use_gram[c] && gram_prepare(b->cfg[c].gp)) return -1;
   if (b->prec == WLG_FP64)
-    build_ops<double>(b);
+    build_ops<double>(b, phase);
   else
-    build_ops<float>(b);
-  pool_free(b, b->tables);
-  if (pool_alloc(b, &b->tables, std::max<size_t>(256, b->host_tables.size()))) {
+    build_ops<float>(b, phase);
+  pool_free(b, P.tables);
+  if (pool_alloc(b, &P.tables, std::max<size_t>(256, P.host_tables.size()))) {
     set_error("batch: cannot allocate the argument tables");
     return -1;
   }
-  WLG_CUDA(cudaMemcpyAsync(b->tables, b->host_tables.data(), b->host_tables.size(),
+  WLG_CUDA(cudaMemcpyAsync(P.tables, P.host_tables.data(), P.host_tables.size(),
                            cudaMemcpyHostToDevice, b->st));
   WLG_CUDA(cudaStreamSynchronize(b->st));  // host_tables may change after this
-  b->built = true;
+  P.built = true;
   return 0;
 }
 
-// capture the pipeline into a graph (nothing executes during capture)
-int capture(wlg_batch* b) {
+// capture one phase into a graph (nothing executes during capture)
+int capture(wlg_batch* b, int phase) {
+  wlg_batch::Phase& P = b->ph[phase];
   WLG_CUDA(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
-  int rc = b->prec == WLG_FP64 ? issue<double>(b) : issue<float>(b);
+  int rc = b->prec == WLG_FP64 ? issue<double>(b, phase) : issue<float>(b, phase);
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(b->st, &g);
-  if (rc || e != cudaSuccess) {
+  if (rc < 0 || e != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
     set_error("batch: graph capture failed: %s", cudaGetErrorString(e));
     cudaGetLastError();
     return -1;
   }
-  b->graph = g;
-  WLG_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
+  P.graph = g;
+  WLG_CUDA(cudaGraphInstantiate(&P.exec, g, 0));
   return 0;
 }
 
+void unbuild_phase(wlg_batch* b, int phase) {
+  wlg_batch::Phase& P = b->ph[phase];
+  if (P.exec) cudaGraphExecDestroy(P.exec);
+  if (P.graph) cudaGraphDestroy(P.graph);
+  pool_free(b, P.tables);
+  P.exec = nullptr;
+  P.graph = nullptr;
+  P.built = false;
+}
+
 void unbuild(wlg_batch* b) {
-  if (b->exec) cudaGraphExecDestroy(b->exec);
-  if (b->graph) cudaGraphDestroy(b->graph);
-  pool_free(b, b->tables);
-  b->exec = nullptr;
-  b->graph = nullptr;
-  b->built = false;
+  unbuild_phase(b, 0);
+  unbuild_phase(b, 1);
+}
+
+// runs one phase: its graph, or its ops directly the first time (then
+// captured); returns the kernels launched or -1
+int run_phase(wlg_batch* b, int phase) {
+  wlg_batch::Phase& P = b->ph[phase];
+  if (build(b, phase)) return -1;
+  if (P.exec) {
+    WLG_CUDA(cudaGraphLaunch(P.exec, b->st));
+  } else {
+    const int k = b->prec == WLG_FP64 ? issue<double>(b, phase) : issue<float>(b, phase);
+    if (k < 0) return -1;
+    P.kernels = k;
+  }
+  return P.kernels;
 }
 
 }  // namespace
@@ -892,41 +957,47 @@ int wlg_batch_run(wlg_batch* b) {
     return -1;
   }
   WLG_CUDA(cudaSetDevice(b->dev));
-  if (build(b)) return -1;
+  const size_t n = b->cfg.size();
   WLG_CUDA(cudaEventRecord(b->ev0, b->st));
-  if (b->exec) {
-    WLG_CUDA(cudaGraphLaunch(b->exec, b->st));
-  } else {
-    int rc = b->prec == WLG_FP64 ? issue<double>(b) : issue<float>(b);
-    if (rc) return -1;
+  // phase 0: smearing and the gauge chains
+  const int k0 = run_phase(b, 0);
+  if (k0 < 0) return -1;
+  const bool captured0 = b->ph[0].exec != nullptr;
+  WLG_CUDA(cudaStreamSynchronize(b->st));
+  // the temporal-gauge form for the lattices whose g is near unitary, the
+  // carried lines for the others (the rule of a single context)
+  std::vector<char> use(n, 0);
+  for (size_t c = 0; c < n; c++) {
+    if (!b->cfg[c].gram) continue;
+    double dev;
+    memcpy(&dev, b->dev_host + c, sizeof(dev));
+    use[c] = dev <= kGramMaxDeviation;
   }
+  if (use != b->use_gram) {
+    unbuild_phase(b, 1);
+    b->use_gram = use;
+  }
+  const int k1 = run_phase(b, 1);
+  if (k1 < 0) return -1;
+  const bool captured1 = b->ph[1].exec != nullptr;
   WLG_CUDA(cudaEventRecord(b->ev1, b->st));
   WLG_CUDA(cudaStreamSynchronize(b->st));
   cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
+  b->kernels = k0 + k1;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_error("batch_run: %s", cudaGetErrorString(e));
     return -1;
   }
-  for (size_t c = 0; c < b->cfg.size(); c++) {
-    if (!b->cfg[c].gram) continue;
-    double dev;
-    memcpy(&dev, b->dev_host + c, sizeof(dev));
-    if (!(dev <= 0.25)) {
-      set_error("batch_run: configuration %zu: |g g^dag - 1| = %g along time, the temporal-gauge "
-                "form does not apply (a carried-line shape, wlg_batch_set_contract_shape, "
-                "measures it)", c, dev);
-      return -1;
-    }
-  }
   bool bulk = false;
-  for (const Cfg& f : b->cfg) bulk = bulk || (!f.gram && f.cp.variant == 7);
+  for (size_t c = 0; c < n; c++) bulk = bulk || (!b->use_gram[c] && b->cfg[c].cp.variant == 7);
   if (bulk && contract_stage_failed() != 0) {
     set_error("batch_run: the contraction's staged-line copies did not arrive in time");
     return -1;
   }
-  // the first run executed the kernels directly; later runs replay a graph
-  if (b->use_graph && !b->exec && capture(b)) return -1;
+  // a phase that ran its ops directly is captured for the next runs
+  if (b->use_graph && !captured0 && capture(b, 0)) return -1;
+  if (b->use_graph && !captured1 && capture(b, 1)) return -1;
   return 0;
 }
 

@@ -409,7 +409,7 @@ static int do_loops_gram(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
     WLG_CUDA(cudaStreamSynchronize(c->st));
     memcpy(&dev, &bits, sizeof(dev));
   }
-  if (!(dev <= 0.25)) return 1;
+  if (!(dev <= kGramMaxDeviation)) return 1;
   if (ensure(c->gUh, nb) || ensure(c->gB, nb) || ensure(c->gA, na) ||
       ensure(c->partial, gp.partial_elems * sizeof(T)) || ensure(c->wl, sizeof(double) * nwl))
     return -1;
@@ -423,8 +423,10 @@ static int do_loops_gram(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
   const double* hinv = (const double*)c->gH.p;
   {
     ProfScope ps(c, "gauge");
-    gauge_first<T>(g, gp, msl, (const T2*)c->levels.p, (const double*)c->gG.p, hinv, uh, bl, al,
-                   c->st);
+    // the A lines of length 1 from the stored B lines, as a batch makes them
+    gauge_first<T>(g, gp, msl, (const T2*)c->levels.p, (const double*)c->gG.p, hinv, uh, bl,
+                   nullptr, c->st);
+    gram_line_step<T>(g, gp, msl, 1, uh, hinv, bl, al, c->st);
   }
   for (int r = 0; r < p->mwlr; r++) {
     const int R = r + 1;

@@ -630,23 +630,24 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64,
   if ((size_t)3 * msl * p.A * esz / 16 >= (size_t)kNoRow) return false;
   p.block = ((p.BX * p.NG + 31) / 32) * 32;
   p.nchunks = 3 * p.ntile * 18 * (32 * esz / 128);
-  // about 16 waves of blocks, 32 to 512 chunks per block: a bounded run of
-  // FP32 sums per partial
-  const long long target = 16LL * num_sms();
-  long long cpc = ((long long)p.nchunks * p.nblk + target - 1) / target;
-  if (cpc < 32) cpc = 32;
-  if (cpc > 512) cpc = 512;
-  if (!fp64) {
-    // FP32 sums: the rounding error of one partial grows with its run of
-    // n = cpc x 32 products, and the relative error of W after the FP64
-    // sum of the partials as n / sqrt(all products); a run of at most
-    // 2 sqrt(nchunks / 32) chunks keeps it at one level (about 1e-7 of W on
-    // the test lattices and at 32^3x64) for small and large lattices
-    const long long acc_cap = (long long)(2.0 * std::sqrt((double)p.nchunks / 32.0));
-    cpc = std::max(1LL, std::min(cpc, acc_cap));
-  }
+  // column chunks per block: as many as the precision allows (at most 512;
+  // FP32 at most 2 sqrt(nchunks / 32): the rounding error of one FP32
+  // partial grows with its run of n = cpc x 32 products and the relative
+  // error of W after the FP64 sum of the partials as n / sqrt(all
+  // products), so this keeps it at one level, about 1e-7 of W, on small and
+  // large lattices); then the splits rounded so that the blocks fill whole
+  // waves of the SMs
+  long long cmax = 512;
+  if (!fp64) cmax = std::min(cmax, (long long)(2.0 * std::sqrt((double)p.nchunks / 32.0)));
+  if (tune->cpc > 0) cmax = tune->cpc;
+  if (cmax < 1) cmax = 1;
+  const long long slots = (long long)num_sms() * p.occ;
+  const long long total = (long long)p.nchunks * p.nblk;
+  long long waves = (total + cmax * slots - 1) / (cmax * slots);
+  long long nsplit = std::max(1LL, (waves * slots) / p.nblk);
+  long long cpc = (p.nchunks + nsplit - 1) / nsplit;
   if (tune->cpc > 0) cpc = tune->cpc;
-  p.cpc = (int)cpc;
+  p.cpc = (int)std::max(1LL, std::min(cpc, cmax));
   p.nsplit = (p.nchunks + p.cpc - 1) / p.cpc;
   p.partial_elems = (size_t)p.nsplit * N0 * mwlt * msl * msl;
   return true;

@@ -146,6 +146,10 @@ struct GramTuning {
 };
 bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64,
                const GramTuning* tune = nullptr);
+// largest |g g^dag - 1| along time for which the form is used: beyond it
+// (links smeared without a converged projection) H^-1 would amplify rounding
+// and the carried-line form measures
+constexpr double kGramMaxDeviation = 0.25;
 // The gauge field g and H^-1 = (g g^dag)^-1 (FP64 slabs of A doubles each)
 // from the temporal links u0; *dev (device) receives max |g g^dag - 1| as the
 // bits of a non-negative double (the form is not used when it exceeds 1/4).
