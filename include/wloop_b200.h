@@ -289,8 +289,9 @@ int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
 int wlg_set_contract_tuning(wlg_ctx* ctx, int variant, int G, int SB, int nCB, int block);
 /* The contraction form the last measurement on ctx used (0: none yet). */
 int wlg_contract_form(wlg_ctx* ctx, int* form);
-/* Shape of the temporal-gauge form's Gram kernel (0: automatic): occ blocks
- * per SM (1: one block of up to 256 threads, 2: two of up to 192), ord the
+/* Shape of the temporal-gauge form's Gram kernel (0: automatic): occ the
+ * occupancy variant (1: one block of up to 256 threads per SM, 2: two of up
+ * to 192, 3: one of up to 384, where a kernel exists), ord the
  * order of its FMAs (1: dot-product chains, 2: one component at a time),
  * bx an upper bound on the start slices per block, stages the copy pipeline
  * depth (2-4), cpc the column chunks per block.  Results do not depend on

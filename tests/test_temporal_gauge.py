@@ -13,7 +13,8 @@ through the last slice are exact zeros.  Here that restatement, in numpy on
 the oracle's own smearing levels, reproduces the oracle's Wilson loops: the
 device form in wloop_b200/csrc/gram.cu computes the same quantity.  The
 approximate SU(3) projection leaves the smeared links unitary only to about
-1e-8 (4 iterations), so the factors H^-1 are needed for FP64 agreement.
+1e-8 (4 iterations, smooth fields), so the factors H^-1 are needed for FP64
+agreement.
 """
 import numpy as np
 import pytest

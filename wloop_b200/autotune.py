@@ -185,10 +185,11 @@ def _as_batch(shape: Shape):
 # ---------------------------------------------------------------------------
 def gram_shapes(prec: str):
     """(occ, ord, bx, stages, cpc) candidates: the kernel variants (one block
-    of 256 or two of 192 threads per SM; dot-product chains or one component
-    at a time), start slices per block and pipeline depth; cpc 0 = the plan's."""
+    of 256, two of 192 or one of 384 threads per SM; dot-product chains or
+    one component at a time), start slices per block and pipeline depth;
+    cpc 0 = the plan's."""
     bxs = (32, 22, 16) if prec == "mixed" else (0, 16, 8)
-    return [(o, r, bx, st, 0) for o in (1, 2) for r in (1, 2) for bx in bxs for st in (0, 2)]
+    return [(o, r, bx, st, 0) for o in (1, 2, 3) for r in (1, 2) for bx in bxs for st in (0, 2)]
 
 
 def gram_sweep(ctx, parms, prec: str, shapes=None, reps: int = 2):

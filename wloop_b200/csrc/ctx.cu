@@ -1131,7 +1131,7 @@ void* wlg_stream(wlg_ctx* c) { return c ? (void*)c->st : nullptr; }
 
 int wlg_set_gram_tuning(wlg_ctx* c, int occ, int ord, int bx, int stages, int cpc) {
   CTX_BEGIN(c);
-  if (occ < 0 || occ > 2 || ord < 0 || ord > 2 || bx < 0 || stages < 0 || stages > 4 ||
+  if (occ < 0 || occ > 3 || ord < 0 || ord > 2 || bx < 0 || stages < 0 || stages > 4 ||
       stages == 1 || cpc < 0) {
     set_error("bad temporal-gauge tuning (occ %d, ord %d, bx %d, stages %d, cpc %d)", occ, ord,
               bx, stages, cpc);

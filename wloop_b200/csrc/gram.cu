@@ -6,7 +6,7 @@
 // is the trace of a closed loop.  With g(x0,xs) = U0(0,xs) U0(1,xs) ...
 // U0(x0-1,xs) the temporal line is exactly L_T(x) = g(x0)^-1 g(x0+T) (the
 // smeared links need not be exactly unitary: the approximate projection
-// leaves them unitary to about 1e-8), and the term becomes
+// leaves them unitary only approximately), and the term becomes
 //     Re tr[ A_s1(x0,xs) B_s2(x0+T,xs)^dag ],
 //     B(x) = g(x) S(x) g(x+Rk)^dag,   A(x) = H(x)^-1 B(x) H(x+Rk)^-1,   H = g g^dag
 // (A = B for unitary links): a real dot product of the 18 numbers of two
@@ -22,8 +22,9 @@
 // with VA, VB the matrices whose rows are (slice, level) and whose columns
 // are (site, direction, component): 36 msl^2 flops per site and (T,R)
 // instead of the 2 msl M + 36 msl^2 of carrying the temporal lines (M = 198).
-// If g is far from unitary (no projection: max |H - 1| > 1/4) the form is
-// not used, since H^-1 would amplify rounding; the caller checks.
+// If g is far from unitary (max |H - 1| > 1/4: no projection, or one that
+// has not converged on a rough field) the form is not used, since H^-1 would
+// amplify rounding; the caller checks.
 //
 // Slab layout (this file only): a field over the unrolled volume Nu x vs,
 // one array per (level, direction), of element type E (float, double):
@@ -358,9 +359,13 @@ __device__ __forceinline__ void gcp_wait(int n) {
 
 constexpr int kRowBytes = 128;
 // occupancy variants: OCC 1 = one block of up to 256 threads per SM (255
-// registers a thread), OCC 2 = two blocks of up to 192 threads (170 registers)
-__host__ __device__ constexpr int gram_threads(int occ) { return occ == 2 ? 192 : 256; }
-constexpr int kMaxGramThreads = 256;
+// registers a thread), OCC 2 = two blocks of up to 192 threads (170
+// registers), OCC 3 = one block of up to 384 threads (170 registers)
+__host__ __device__ constexpr int gram_threads(int occ) {
+  return occ == 2 ? 192 : (occ == 3 ? 384 : 256);
+}
+__host__ __device__ constexpr int gram_blocks_per_sm(int occ) { return occ == 2 ? 2 : 1; }
+constexpr int kMaxGramThreads = 384;
 constexpr unsigned kNoRow = 0xffffffffu;
 
 struct GramArgs {
@@ -378,7 +383,7 @@ __host__ __device__ __forceinline__ int round8(int v) { return (v + 7) & ~7; }
 // chains of one B vector interleave); ORD 1: one component at a time over
 // the L sums of a B vector
 template <class E, int L, int TQ, int OCC, int ORD>
-__global__ void __launch_bounds__(gram_threads(OCC), OCC) k_gram(GramArgs P) {
+__global__ void __launch_bounds__(gram_threads(OCC), gram_blocks_per_sm(OCC)) k_gram(GramArgs P) {
   constexpr int KW = 128 / (int)sizeof(E);
   constexpr int VN = GVec<E>::N;
   typedef typename GVec<E>::t V;
@@ -532,13 +537,15 @@ __global__ void __launch_bounds__(256) k_gram_reduce(const E* __restrict__ parti
 // ---------------------------------------------------------------------------
 // Instantiations (element, levels L, extents per thread TQ, occupancy OCC,
 // FMA order ORD).  The first entry of a (type, L) pair is its default; the
-// others are tuning candidates.  FP32 keeps at most 128 sums per thread,
-// FP64 at most 64 doubles in OCC 2 (170 registers) and 72 in OCC 1.
+// others are tuning candidates.  FP32 keeps at most 128 sums per thread
+// (72 in OCC 3), FP64 at most 64 doubles in OCC 2 (170 registers) and 72 in
+// OCC 1.
 // ---------------------------------------------------------------------------
 #define WLG_GRAM_VARIANTS(X)                                                                   \
   X(float, 1, 8, 1, 0) X(float, 2, 8, 1, 0) X(float, 3, 6, 1, 0) X(float, 4, 6, 1, 0)           \
   X(float, 4, 4, 1, 0) X(float, 5, 4, 1, 0) X(float, 6, 3, 1, 0) X(float, 6, 3, 1, 1)           \
-  X(float, 6, 3, 2, 0) X(float, 6, 3, 2, 1) X(float, 7, 2, 1, 0) X(float, 8, 2, 1, 0)           \
+  X(float, 6, 3, 2, 0) X(float, 6, 3, 2, 1) X(float, 6, 2, 3, 0) X(float, 4, 4, 3, 0)           \
+  X(float, 7, 2, 1, 0) X(float, 8, 2, 1, 0)                                                     \
   X(double, 1, 8, 2, 1) X(double, 2, 6, 2, 1) X(double, 3, 4, 2, 1) X(double, 4, 3, 2, 1)       \
   X(double, 4, 2, 2, 1) X(double, 5, 2, 2, 1) X(double, 6, 1, 2, 1) X(double, 6, 1, 2, 0)       \
   X(double, 6, 2, 1, 0) X(double, 6, 2, 1, 1) X(double, 7, 1, 2, 1) X(double, 8, 1, 2, 1)
@@ -608,7 +615,7 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64,
   const int bxmax = std::min(cap / p.NG, tune->bx > 0 ? tune->bx : N0);
   // the fewest start-slice blocks whose rows fit two stages in the shared
   // memory of one block (half an SM's for two blocks per SM)
-  const size_t lim = p.occ == 2 ? 113 * 1024 : 227 * 1024;
+  const size_t lim = gram_blocks_per_sm(p.occ) == 2 ? 113 * 1024 : 227 * 1024;
   for (int nblk = (N0 + bxmax - 1) / bxmax; nblk <= N0; nblk++) {
     const int BX = (N0 + nblk - 1) / nblk;
     const int nrows = msl * (round8(BX) + round8(BX + mwlt - 1));
@@ -641,7 +648,7 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64,
   if (!fp64) cmax = std::min(cmax, (long long)(2.0 * std::sqrt((double)p.nchunks / 32.0)));
   if (tune->cpc > 0) cmax = tune->cpc;
   if (cmax < 1) cmax = 1;
-  const long long slots = (long long)num_sms() * p.occ;
+  const long long slots = (long long)num_sms() * gram_blocks_per_sm(p.occ);
   const long long total = (long long)p.nchunks * p.nblk;
   long long waves = (total + cmax * slots - 1) / (cmax * slots);
   long long nsplit = std::max(1LL, (waves * slots) / p.nblk);
