@@ -105,7 +105,7 @@ def test_budget_counts_memory_the_batch_pool_keeps():
 
 # a request that takes the GPU about a tenth of a second
 BIG_N = (64, 32, 32, 32)
-BIG_P = WloopParms(msl=4, nss=[0, 10, 10, 10], mwlt=8, mwlr=6, op_smear=APE, alpha_ape=0.5,
+BIG_P = WloopParms(msl=4, nss=[0, 10, 10, 10], mwlt=16, mwlr=12, op_smear=APE, alpha_ape=0.5,
                    proj_iter=4)
 
 
