@@ -101,6 +101,13 @@ struct wlg_batch {
   bool use_graph = true;       // capture each phase after its first run and replay it
   int tG = 0, tSB = 0, tBlock = 0, tNCB = 0;  // contraction shape override (tuning)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // the temporal-gauge lattices of phase 1 run on these streams, lattice c
+  // on side[c % kSide], forked from and joined back into st (inside the
+  // captured graph, parallel branches), so the small per-lattice kernels of
+  // different lattices overlap
+  static constexpr int kSide = 4;
+  cudaStream_t side[kSide] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t fork = nullptr, join[kSide] = {nullptr, nullptr, nullptr, nullptr};
   float last_ms = 0.f;
   int kernels = 0;
 };
@@ -493,7 +500,24 @@ template <class T> void build_ops(wlg_batch* b, int phase) {
 template <class T> int issue(wlg_batch* b, int phase) {
   int kernels = 0;
   const char* tables = b->ph[phase].tables;
+  bool forked = false;
+  auto lattice_stream = [&](int c) -> cudaStream_t {
+    return b->side[0] ? b->side[c % wlg_batch::kSide] : b->st;
+  };
   for (const Op& op : b->ph[phase].ops) {
+    const bool gram_op = op.kind == OP_GRAM_PREP || op.kind == OP_GRAM_R;
+    if (gram_op && !forked && b->side[0]) {
+      WLG_CUDA(cudaEventRecord(b->fork, b->st));
+      for (int k = 0; k < wlg_batch::kSide; k++) WLG_CUDA(cudaStreamWaitEvent(b->side[k], b->fork, 0));
+      forked = true;
+    }
+    if (op.kind == OP_D2H && forked) {
+      for (int k = 0; k < wlg_batch::kSide; k++) {
+        WLG_CUDA(cudaEventRecord(b->join[k], b->side[k]));
+        WLG_CUDA(cudaStreamWaitEvent(b->st, b->join[k], 0));
+      }
+      forked = false;
+    }
     switch (op.kind) {
       case OP_SMEAR:
         smear_batch<T>(op.stage, (const SArgs<T>*)(tables + op.tab),
@@ -535,13 +559,14 @@ template <class T> int issue(wlg_batch* b, int phase) {
         typedef typename V2<T>::t T2;
         char* r = b->arena + f.region;
         const size_t es = elem_bytes(b);
+        cudaStream_t ls = lattice_stream(op.cfg);
         gauge_first<T>(f.g, f.gp, f.p.msl, (const T2*)(r + 6 * f.D * es),
                        (const double*)(b->arena + f.gG), (const double*)(b->arena + f.gH),
-                       (T*)(b->arena + f.gUh), (T*)(b->arena + f.gB), nullptr, b->st);
+                       (T*)(b->arena + f.gUh), (T*)(b->arena + f.gB), nullptr, ls);
         // the A lines of length 1 (they may overwrite the level store)
         gram_line_step<T>(f.g, f.gp, f.p.msl, 1, (const T*)(b->arena + f.gUh),
                           (const double*)(b->arena + f.gH), (T*)(b->arena + f.gB),
-                          (T*)(b->arena + f.gA), b->st);
+                          (T*)(b->arena + f.gA), ls);
         kernels += 2;
         break;
       }
@@ -549,14 +574,15 @@ template <class T> int issue(wlg_batch* b, int phase) {
         const Cfg& f = b->cfg[op.cfg];
         T* bl = (T*)(b->arena + f.gB);
         T* al = (T*)(b->arena + f.gA);
+        cudaStream_t ls = lattice_stream(op.cfg);
         if (op.R >= 2) {
           gram_line_step<T>(f.g, f.gp, f.p.msl, op.R, (const T*)(b->arena + f.gUh),
-                            (const double*)(b->arena + f.gH), bl, al, b->st);
+                            (const double*)(b->arena + f.gH), bl, al, ls);
           kernels++;
         }
-        gram_contract<T>(f.g, f.gp, f.p.mwlt, al, bl, (T*)(b->pbuf + f.gpartial), b->st);
+        gram_contract<T>(f.g, f.gp, f.p.mwlt, al, bl, (T*)(b->pbuf + f.gpartial), ls);
         gram_reduce<T>(f.g, f.gp, f.bc, f.p.mwlt, f.p.mwlr, op.R - 1,
-                       (const T*)(b->pbuf + f.gpartial), (double*)(b->arena + f.wl), b->st);
+                       (const T*)(b->pbuf + f.gpartial), (double*)(b->arena + f.wl), ls);
         kernels += 2;
         break;
       }
@@ -833,6 +859,19 @@ int wlg_batch_create(int nconf, const int* dims, const int* bcs, const wlg_wloop
   // the allocations are ordered on the batch's stream; complete them before
   // the host hands the buffers to copies on other streams
   WLG_CUDA(cudaStreamSynchronize(b->st));
+  for (int k = 0; k < wlg_batch::kSide; k++) {
+    if (cudaStreamCreateWithFlags(&b->side[k], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming) != cudaSuccess) {
+      set_error("batch_create: cannot create the lattice streams");
+      wlg_batch_destroy(b);
+      return -1;
+    }
+  }
+  if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
+    set_error("batch_create: cannot create the lattice streams");
+    wlg_batch_destroy(b);
+    return -1;
+  }
   cudaEventCreate(&b->ev0);
   cudaEventCreate(&b->ev1);
   *out = b;
@@ -854,6 +893,14 @@ int wlg_batch_destroy(wlg_batch* b) {
   if (b->dev_host) cudaFreeHost(b->dev_host);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
+  for (int k = 0; k < wlg_batch::kSide; k++) {
+    if (b->side[k]) {
+      cudaStreamSynchronize(b->side[k]);
+      cudaStreamDestroy(b->side[k]);
+    }
+    if (b->join[k]) cudaEventDestroy(b->join[k]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
   return 0;
