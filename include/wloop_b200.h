@@ -280,8 +280,9 @@ int wlg_set_contract_shape(wlg_ctx* ctx, int G, int nCB, int block);
  * which the temporal lines are unit matrices (g(x0) = U0(0) ... U0(x0-1),
  * exact for links that are unitary only approximately) and evaluates every
  * loop as a dot product of two transformed lines: a banded Gram product.  It
- * is used for every measurement unless another form is asked for here, and
- * it falls back to the default carried-line form (7 FP64, 10 mixed) when
+ * is used for every measurement on lattices of at least 32768 sites unless
+ * another form is asked for here (variant 11 asks for it on any lattice),
+ * and it falls back to the default carried-line form (7 FP64, 10 mixed) when
  * g g^dag differs from 1 by more than 1/4 anywhere (links smeared without
  * projection) or when msl and mwlt do not fit its kernel; wlg_contract_form
  * tells which form ran.  After it the spatial lines that

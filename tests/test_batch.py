@@ -178,3 +178,34 @@ def test_tune_context_picks_a_shape_with_the_same_result(tmp_path, monkeypatch):
         got = c.measure(p)
     assert shape in autotune.candidates(4, False, False)
     assert np.abs(got - base).max() <= 1e-6 * np.abs(base).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_batch_temporal_gauge_lattices_equal_contexts(prec):
+    """Lattices of at least 32768 sites run the temporal-gauge form in a
+    batch as in a context (bit for bit), beside a small lattice that runs the
+    carried lines in both."""
+    items = [((8, 16, 16, 16), 3, WloopParms(msl=2, nss=[0, 2], mwlt=4, mwlr=3, op_smear=APE,
+                                              alpha_ape=0.5, proj_iter=4)),
+             ((16, 16, 16, 8), 0, WloopParms(msl=3, nss=[0, 1, 2], mwlt=5, mwlr=2, op_smear=APE,
+                                              alpha_ape=0.5, proj_iter=4)),
+             ((8, 4, 6, 4), 3, WloopParms(msl=2, nss=[0, 2], mwlt=3, mwlr=2, op_smear=APE,
+                                          alpha_ape=0.5, proj_iter=4))]
+    fields = [generate_links(n, bc, 970 + i, 0.25) for i, (n, bc, _) in enumerate(items)]
+    singles, forms = [], []
+    for (n, bc, p), u in zip(items, fields):
+        with Context(n, bc, prec) as c:
+            c.upload(u)
+            singles.append(c.measure(p))
+            forms.append(c.contract_form)
+    assert forms[0] == 11 and forms[1] == 11 and forms[2] != 11
+    with Batch(items, prec) as b:
+        for i, u in enumerate(fields):
+            b.upload(i, u)
+        b.snapshot()
+        b.run()
+        b.restore()
+        b.run()  # graph replay
+        for i in range(len(items)):
+            assert np.array_equal(b.result(i), singles[i]), f"config {i}"

@@ -381,12 +381,14 @@ def test_prefetched_upload(prec):
         assert np.array_equal(c.measure(p), ref1)
 
 
-@pytest.mark.parametrize("prec,form", [("fp64", 0), ("fp64", 3), ("mixed", 0), ("mixed", 3)])
+@pytest.mark.parametrize("prec,form", [("fp64", 0), ("fp64", 3), ("fp64", 11), ("mixed", 0),
+                                       ("mixed", 3), ("mixed", 11)])
 def test_lines_left_by_the_measurement(prec, form):
     """The spatial lines a measurement leaves (get_pus slots msl..2msl-1) are
     the products of mwlr level links along each direction, whether the
     contraction computed them (fourth-form family) or the line-step stage did
-    (third form)."""
+    (third form), or they are rebuilt from the level store after a
+    temporal-gauge measurement (form 11)."""
     n, bc, p = CASES[1]
     u = generate_links(n, bc, 77, 0.25)
     with Context(n, bc, prec) as c:

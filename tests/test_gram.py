@@ -1,8 +1,9 @@
 """The temporal-gauge contraction form (wloop_b200/csrc/gram.cu) on the GPU.
 
-It is every context's default: the lattices of the parity cases run it
+It is a context's default on lattices of at least 32768 sites and can be
+asked for on any (contraction form 11): on the lattices of the parity cases
 (odd extents, time slices that are not whole 32-site tiles, 1 to 8 levels,
-open and periodic time, the largest loops the parameters allow), it agrees
+open and periodic time, the largest loops the parameters allow) it agrees
 with the carried-temporal-line form and with the FP64 oracle at the same
 bars (FP64: 1e-12 of max(|W|, sum|terms|/norm); mixed: 1e-6 plain
 relative), the lattices whose start slices need several blocks and whose
@@ -44,12 +45,35 @@ def _check(prec, got, ref, ref_abs):
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 @pytest.mark.parametrize("case", PROJECTED)
-def test_default_form_is_the_temporal_gauge(case, prec):
+def test_form_choice(case, prec):
+    """Below 32768 sites the carried lines are the default; form 11 asks for
+    the temporal gauge."""
     n, bc, p = CASES[case]
     with Context(n, bc, prec) as c:
         c.generate(900 + case, 0.25)
+        c.snapshot()
+        c.measure(p)
+        assert c.contract_form not in (0, 11)
+        c.set_contract_tuning(variant=11)
+        c.restore()
         c.measure(p)
         assert c.contract_form == 11
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_default_on_a_large_lattice(prec):
+    """16^3x8 (32768 sites) runs the temporal gauge by default and agrees
+    with the oracle."""
+    n, bc = (8, 16, 16, 16), 3
+    p = WloopParms(msl=2, nss=[0, 2], mwlt=4, mwlr=2, op_smear=APE, alpha_ape=0.5, proj_iter=4)
+    u = generate_links(n, bc, 960, 0.25)
+    uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
+    ref, ref_abs = O.wloop_sum(n, bc, uh, p, want_abs=True)
+    with Context(n, bc, prec) as c:
+        c.upload(u)
+        got = c.measure(p)
+        assert c.contract_form == 11
+    _check(prec, got, ref, ref_abs)
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
@@ -60,6 +84,7 @@ def test_temporal_gauge_against_carried_lines(case, prec):
     uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
     ref, ref_abs = O.wloop_sum(n, bc, uh, p, want_abs=True)
     with Context(n, bc, prec) as c:
+        c.set_contract_tuning(variant=11)
         c.upload(u)
         c.snapshot()
         gram = c.measure(p)
@@ -83,6 +108,7 @@ def test_several_blocks_and_splits(wide, prec):
     uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
     ref, ref_abs = O.wloop_sum(n, bc, uh, p, want_abs=True)
     with Context(n, bc, prec) as c:
+        c.set_contract_tuning(variant=11)
         c.upload(u)
         got = c.measure(p)
         assert c.contract_form == 11
@@ -103,6 +129,7 @@ def test_unprojected_field_falls_back(prec):
     uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
     ref, ref_abs = O.wloop_sum(n, bc, uh, p, want_abs=True)
     with Context(n, bc, prec) as c:
+        c.set_contract_tuning(variant=11)  # asked for, not applicable
         c.upload(u)
         got = c.measure(p)
         assert c.contract_form not in (0, 11)
@@ -122,6 +149,7 @@ def test_kernel_variants_agree_bit_for_bit(prec):
     (for a fixed number of column chunks per block)."""
     n, bc, p = WIDE[0]
     with Context(n, bc, prec) as c:
+        c.set_contract_tuning(variant=11)
         c.generate(950, 0.3)
         c.snapshot()
         c.set_gram_tuning(cpc=2)

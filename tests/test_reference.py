@@ -171,8 +171,11 @@ def test_reference_reproduces_c1_fixture():
 # GPU against the reference
 # ---------------------------------------------------------------------------
 @pytest.mark.gpu
+@pytest.mark.parametrize("form", [0, 11])
 @pytest.mark.parametrize("case", range(len(CASES)))
-def test_gpu_matches_reference(case):
+def test_gpu_matches_reference(case, form):
+    """The default form (the carried lines on these small lattices) and the
+    temporal-gauge form (11) against the reference."""
     from wloop_b200 import Context
     n, bc, p = CASES[case]
     ref = need(n)
@@ -183,6 +186,7 @@ def test_gpu_matches_reference(case):
     uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
     _, want_abs = O.wloop_sum(n, bc, uh, p, want_abs=True)
     with Context(n, bc, "fp64") as c:
+        c.set_contract_tuning(variant=form)
         c.upload(u)
         got = c.measure(p)
     err = scaled_err(got, want, want_abs)
@@ -192,6 +196,7 @@ def test_gpu_matches_reference(case):
     assert err <= 1e-12
     assert rel.max() <= 1e-12  # these fields hold no near-zero W
     with Context(n, bc, "mixed") as c:
+        c.set_contract_tuning(variant=form)
         c.upload(u)
         gm = c.measure(p)
     assert np.all(gm[~nz] == 0.0)

@@ -11,8 +11,9 @@
 // has finished for every lattice before the first sweep writes there).  The
 // contraction forms 4-7 write the next R's lines themselves, alternating
 // between the two line buffers; the third form runs a line-step stage.
-// Configurations whose smearing projects (proj_iter >= 3) run the
-// temporal-gauge form (gram.cu) instead, one launch per lattice and stage
+// Configurations of at least kGramMinSites sites whose smearing projects
+// (proj_iter >= 3) run the temporal-gauge form (gram.cu) instead, one launch
+// per lattice and stage
 // inside the same graph: its g and H^-1 take the APE ping-pong slots, its A
 // lines the level store (dead once the first lines exist), its recursion
 // links and B lines start at the first line buffer, the region grown where
@@ -643,7 +644,7 @@ void layout(wlg_batch* b) {
     // second lines 3 msl, or the HYP scratch (24), whichever is larger
     size_t rdirs = std::max<size_t>(24, 12 + 9 * (size_t)f.p.msl);
     size_t rbytes = rdirs * f.D * es;
-    f.gram_ok = f.p.proj_iter >= 3 &&
+    f.gram_ok = f.p.proj_iter >= 3 && (long long)f.g.vol >= kGramMinSites &&
                 gram_plan(f.gp, f.g, f.bc, f.p.msl, f.p.mwlt, fp64);
     if (f.gram_ok) {
       // after the smearing: g and H^-1 in the APE ping-pong slots (6 D),

@@ -469,8 +469,9 @@ static int do_loops(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
     }
     contract9_plan(cp, g, msl, p->mwlt);
   }
-  // the temporal-gauge form unless another form is asked for
-  if (c->cVariant == 0 || c->cVariant == 11) {
+  // the temporal-gauge form when asked for, or by default on lattices of at
+  // least kGramMinSites sites
+  if (c->cVariant == 11 || (c->cVariant == 0 && (long long)g.vol >= kGramMinSites)) {
     const int rc = do_loops_gram<T>(c, p, wl_mat);
     if (rc != 1) return rc;
     if (cp.variant == 11) cp = contract_plan(g, msl, p->mwlt, c->prec == WLG_FP64, c->cG, c->cNCB,

@@ -45,6 +45,9 @@
 // fixed order.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "internal.h"
 
@@ -733,13 +736,20 @@ int gram_prepare(const GramPlan& p) {
     return -1;
   }
   // the limit is per kernel, not per plan: the largest any plan may use, so
-  // that plans of other lattices keep launching
+  // that plans of other lattices keep launching; set once per kernel and device
+  static std::mutex mu;
+  static std::set<std::pair<int, void*>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({dev, fn})) return 0;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) !=
       cudaSuccess) {
     set_error("gram: %zu bytes of shared memory per block: %s", p.smem,
               cudaGetErrorString(cudaGetLastError()));
     return -1;
   }
+  done.insert({dev, fn});
   return 0;
 }
 

@@ -150,6 +150,11 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64,
 // (links smeared without a converged projection) H^-1 would amplify rounding
 // and the carried-line form measures
 constexpr double kGramMaxDeviation = 0.25;
+// smallest lattice (sites) on which the form is the default: below it its
+// fixed costs per measurement (the deviation read-back, the gauge chain, two
+// more launches per R) outweigh the arithmetic it saves (8^4: 0.65 against
+// 0.49 ms per measurement); it can still be asked for explicitly
+constexpr long long kGramMinSites = 32768;
 // The gauge field g and H^-1 = (g g^dag)^-1 (FP64 slabs of A doubles each)
 // from the temporal links u0; *dev (device) receives max |g g^dag - 1| as the
 // bits of a non-negative double (the form is not used when it exceeds 1/4).
