@@ -326,10 +326,10 @@ __global__ void __launch_bounds__(128) k_gauge_line_step(Geo g, int Nu, int ntil
 // and the TQ extents T = gq + 1 + NG j (j < TQ): per 16-byte column group it
 // reads the L A-vectors of its slice and, one at a time, the L B-vectors of
 // each partner slice, and advances the L sums of a B vector (the order of
-// the FMAs and the occupancy -- one block of 256 or two of 192 threads per
-// SM -- are kernel variants; the plan picks one per precision).  Lanes of a warp share start slices
-// (broadcast reads), and the partner rows one read of a warp touches span at
-// most 32/NG + NG - 1 consecutive slices.
+// the FMAs and the occupancy -- one block of 256, two of 192 or one of 384
+// threads per SM -- are kernel variants; the plan picks one per precision).
+// Lanes of a warp share start slices (broadcast reads), and the partner rows
+// one read of a warp touches span at most 32/NG + NG - 1 consecutive slices.
 // ---------------------------------------------------------------------------
 template <class E> struct GVec;
 template <> struct GVec<float> {
