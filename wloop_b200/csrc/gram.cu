@@ -39,7 +39,7 @@
 //
 // g, H^-1 and the transformed links are computed in FP64 in both forms (the
 // mixed form stores the links and lines rounded to FP32, as it stores the
-// smeared links); the line products are FP64; the Gram product accumulates
+// smeared links); the line products are in the stored type; the Gram product accumulates
 // in the form's type over a bounded run of columns per block (FP32: a few
 // thousand products) and the per-block partial sums are added in FP64 in a
 // fixed order.
@@ -74,6 +74,29 @@ __device__ __forceinline__ void ld_slab(M3<double>& m, const E* __restrict__ bas
 template <class E>
 __device__ __forceinline__ void st_slab(E* __restrict__ base, size_t tile, int lane,
                                         const M3<double>& m) {
+  E* p = base + tile * kSlabTile + lane;
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    p[(2 * e) * 32] = (E)m.e[e].x;
+    p[(2 * e + 1) * 32] = (E)m.e[e].y;
+  }
+}
+
+// the same in arithmetic type A (loads convert from the stored type S)
+template <class A, class S>
+__device__ __forceinline__ void ld_slab_as(M3<A>& m, const S* __restrict__ base, size_t tile,
+                                           int lane) {
+  const S* p = base + tile * kSlabTile + lane;
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    m.e[e].x = (A)__ldg(p + (2 * e) * 32);
+    m.e[e].y = (A)__ldg(p + (2 * e + 1) * 32);
+  }
+}
+
+template <class E, class A>
+__device__ __forceinline__ void st_slab_from(E* __restrict__ base, size_t tile, int lane,
+                                             const M3<A>& m) {
   E* p = base + tile * kSlabTile + lane;
 #pragma unroll
   for (int e = 0; e < 9; e++) {
@@ -255,8 +278,11 @@ __global__ void __launch_bounds__(128) k_gauge_first(Geo g, int Nu, int ntile, i
 // ---------------------------------------------------------------------------
 // Line step: B(y, j) <- B(y, j) Uh(y, j + (R-1) k) in place (compute_uk_long,
 // wloop.c:207-258, multiplied at the far end), and for the start slices
-// A(y, j) = H^-1(y, j) B(y, j) H^-1(y, j + R k); FP64 products.  With R = 1
-// only A, from the lines of length 1.
+// A(y, j) = H^-1(y, j) B(y, j) H^-1(y, j + R k); products in the stored type
+// (the mixed form's as packed two-lane FP32 FMAs: each line is rounded to
+// FP32 at every step anyway, and FP64 products here cost FP64-pipe time and
+// registers that limited this HBM-bound kernel).  With R = 1 only A, from
+// the lines of length 1.
 // ---------------------------------------------------------------------------
 template <class E>
 __global__ void __launch_bounds__(128) k_gauge_line_step(Geo g, int Nu, int ntile, int msl, int R,
@@ -290,23 +316,23 @@ __global__ void __launch_bounds__(128) k_gauge_line_step(Geo g, int Nu, int ntil
     int x[4];
     coords(g, j, x);  // slice 0: the spatial coordinates of j
     const int n_k = g.n[k + 1];
-    M3<double> a, b, c;
+    M3<E> a, b, c;
     if (R >= 2) {
       const int jr = shift(g, j, x[k + 1], k + 1, (R - 1) % n_k);
-      ld_slab(a, blines + (size_t)q * A, tile, lane);
-      ld_slab(b, uh + (size_t)q * A, slab_tile(y0, ntile, jr >> 5), jr & 31);
+      ld_slab_as(a, blines + (size_t)q * A, tile, lane);
+      ld_slab_as(b, uh + (size_t)q * A, slab_tile(y0, ntile, jr >> 5), jr & 31);
       mul(c, a, b);
-      st_slab(blines + (size_t)q * A, tile, lane, c);
+      st_slab_from(blines + (size_t)q * A, tile, lane, c);
     } else {
-      ld_slab(c, blines + (size_t)q * A, tile, lane);
+      ld_slab_as(c, blines + (size_t)q * A, tile, lane);
     }
     if (start) {
       const int je = shift(g, j, x[k + 1], k + 1, R % n_k);
-      ld_slab(a, Hinv, tile, lane);
+      ld_slab_as(a, Hinv, tile, lane);
       mul(b, a, c);
-      ld_slab(a, Hinv, slab_tile(y0, ntile, je >> 5), je & 31);
+      ld_slab_as(a, Hinv, slab_tile(y0, ntile, je >> 5), je & 31);
       mul(c, b, a);
-      st_slab(alines + (size_t)q * Aa, tile, lane, c);
+      st_slab_from(alines + (size_t)q * Aa, tile, lane, c);
     }
   }
 }
