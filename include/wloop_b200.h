@@ -304,6 +304,14 @@ int wlg_set_gram_tuning(wlg_ctx* ctx, int occ, int ord, int bx, int stages, int 
  * of start slices, stages, chunks per block, column splits, threads per
  * block, shared memory per block in KiB}. */
 int wlg_gram_shape(wlg_ctx* ctx, int msl, int mwlt, int* shape);
+/* The same plan without a context or a GPU (the SM count then defaults to
+ * 148): n the lattice, tune {occ, ord, bx, stages, cpc} or NULL; shape[16] =
+ * {extents per thread, occ, ord, start slices per block, its rows padded to
+ * 8, extent groups, B rows per level, padded to 8, blocks of start slices,
+ * staged rows, stages, threads per block, shared memory bytes per block,
+ * column chunks, chunks per block, column splits}. */
+int wlg_gram_plan_shape(const int n[4], int bc, int msl, int mwlt, int precision,
+                        const int tune[5], long long shape[16]);
 /* The context's CUDA stream (cudaStream_t), for callers that record events. */
 void* wlg_stream(wlg_ctx* ctx);
 /* Number of wloop_b200 kernel launches issued by this process so far. */

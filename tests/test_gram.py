@@ -29,6 +29,12 @@ WIDE = [
                                   op_smear=APE, alpha_ape=0.5, proj_iter=4)),
     ((40, 4, 4, 4), 0, WloopParms(msl=6, nss=[0, 1, 1, 1, 1, 1], mwlt=21, mwlr=3,
                                   op_smear=APE, alpha_ape=0.5, proj_iter=4)),
+    # 7 levels and t <= 49: the rows of one start slice do not fit two stages
+    # in half an SM's shared memory, so FP64 takes its one-block-per-SM kernel
+    ((96, 4, 4, 4), 3, WloopParms(msl=7, nss=[0, 1, 1, 1, 1, 1, 1], mwlt=49, mwlr=2,
+                                  op_smear=APE, alpha_ape=0.5, proj_iter=4)),
+    ((96, 4, 4, 4), 0, WloopParms(msl=7, nss=[0, 1, 1, 1, 1, 1, 1], mwlt=49, mwlr=2,
+                                  op_smear=APE, alpha_ape=0.5, proj_iter=4)),
 ]
 
 
@@ -112,6 +118,8 @@ def test_several_blocks_and_splits(wide, prec):
         c.upload(u)
         got = c.measure(p)
         assert c.contract_form == 11
+        if prec == "fp64" and p.msl == 7:
+            assert c.gram_shape(p.msl, p.mwlt)["occ"] == 1
     _check(prec, got, ref, ref_abs)
 
 

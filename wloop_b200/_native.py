@@ -94,6 +94,7 @@ def _load():
         "wlg_contract_form": (i, [vp, ip]),
         "wlg_set_gram_tuning": (i, [vp, i, i, i, i, i]),
         "wlg_gram_shape": (i, [vp, i, i, ip]),
+        "wlg_gram_plan_shape": (i, [ip, i, i, i, i, ip, C.POINTER(C.c_longlong)]),
         "wlg_launch_count": (C.c_longlong, []),
         "wlg_snapshot": (i, [vp]),
         "wlg_gauge_transform": (i, [vp, u64, d]),

@@ -1159,6 +1159,35 @@ int wlg_gram_shape(wlg_ctx* c, int msl, int mwlt, int* shape) {
   return 0;
 }
 
+int wlg_gram_plan_shape(const int n[4], int bc, int msl, int mwlt, int precision,
+                        const int tune[5], long long shape[16]) {
+  set_error("%s", "");
+  if (!n || !shape || (precision != WLG_FP64 && precision != WLG_MIXED)) {
+    set_error("gram_plan_shape: bad arguments");
+    return -1;
+  }
+  GramTuning t;
+  if (tune) {
+    t.occ = tune[0];
+    t.ord = tune[1];
+    t.bx = tune[2];
+    t.stages = tune[3];
+    t.cpc = tune[4];
+  }
+  GramPlan gp;
+  const bool ok = gram_plan(gp, make_geo(n), bc, msl, mwlt, precision == WLG_FP64, &t);
+  cudaGetLastError();  // a host without a GPU leaves the SM-count query's error behind
+  if (!ok) {
+    set_error("no temporal-gauge plan for msl %d, mwlt %d", msl, mwlt);
+    return -1;
+  }
+  const long long v[16] = {gp.TQ, gp.occ, gp.ord + 1, gp.BX, gp.BXp, gp.NG, gp.NYB, gp.NYBp,
+                           gp.nblk, gp.nrows, gp.stages, gp.block, (long long)gp.smem,
+                           gp.nchunks, gp.cpc, gp.nsplit};
+  for (int i = 0; i < 16; i++) shape[i] = v[i];
+  return 0;
+}
+
 int wlg_contract_form(wlg_ctx* c, int* form) {
   CTX_BEGIN(c);
   if (!form) {

@@ -566,7 +566,8 @@ __global__ void __launch_bounds__(256) k_gram_reduce(const E* __restrict__ parti
 // ---------------------------------------------------------------------------
 // Instantiations (element, levels L, extents per thread TQ, occupancy OCC,
 // FMA order ORD).  The first entry of a (type, L) pair is its default; the
-// others are tuning candidates.  FP32 keeps at most 128 sums per thread
+// others are tuning candidates or serve where the default's rows do not fit
+// its shared memory.  FP32 keeps at most 128 sums per thread
 // (72 in OCC 3), FP64 at most 64 doubles in OCC 2 (170 registers) and 72 in
 // OCC 1.
 // ---------------------------------------------------------------------------
@@ -577,7 +578,8 @@ __global__ void __launch_bounds__(256) k_gram_reduce(const E* __restrict__ parti
   X(float, 7, 2, 1, 0) X(float, 8, 2, 1, 0)                                                     \
   X(double, 1, 8, 2, 1) X(double, 2, 6, 2, 1) X(double, 3, 4, 2, 1) X(double, 4, 3, 2, 1)       \
   X(double, 4, 2, 2, 1) X(double, 5, 2, 2, 1) X(double, 6, 1, 2, 1) X(double, 6, 1, 2, 0)       \
-  X(double, 6, 2, 1, 0) X(double, 6, 2, 1, 1) X(double, 7, 1, 2, 1) X(double, 8, 1, 2, 1)
+  X(double, 6, 2, 1, 0) X(double, 6, 2, 1, 1) X(double, 7, 1, 2, 1) X(double, 8, 1, 2, 1)       \
+  X(double, 7, 1, 1, 1) X(double, 8, 1, 1, 1)
 
 void* gram_kernel(int esize, int L, int TQ, int occ, int ord) {
 #define WLG_GRAM_PICK(ET, LL, TT, OO, RR)                                                     \
@@ -621,45 +623,55 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64,
   p.Aa = (size_t)g.n[0] * p.ntile * kSlabTile;
   GramVariant cand[16];
   const int nc = gram_variants(esz, msl, tune->occ, tune->ord, cand, 16);
-  // the default variant of the level count's first occupancy and order, with
-  // the extents per thread that waste the fewest (ties: the first listed)
-  int best = -1, bw = 1 << 30;
-  for (int c = 0; c < nc; c++) {
-    if (cand[c].occ != cand[0].occ || cand[c].ord != cand[0].ord) continue;
-    const int ng = (mwlt + cand[c].TQ - 1) / cand[c].TQ;
-    const int waste = ng * cand[c].TQ - mwlt;
-    if (waste < bw) {
-      bw = waste;
-      best = c;
-    }
-  }
-  if (best < 0) return false;
-  p.TQ = cand[best].TQ;
-  p.occ = cand[best].occ;
-  p.ord = cand[best].ord;
-  p.NG = (mwlt + p.TQ - 1) / p.TQ;
-  const int cap = gram_threads(p.occ);
-  if (p.NG > cap) return false;
   const int N0 = g.n[0];
-  const int bxmax = std::min(cap / p.NG, tune->bx > 0 ? tune->bx : N0);
-  // the fewest start-slice blocks whose rows fit two stages in the shared
-  // memory of one block (half an SM's for two blocks per SM)
-  const size_t lim = gram_blocks_per_sm(p.occ) == 2 ? 113 * 1024 : 227 * 1024;
-  for (int nblk = (N0 + bxmax - 1) / bxmax; nblk <= N0; nblk++) {
-    const int BX = (N0 + nblk - 1) / nblk;
-    const int nrows = msl * (round8(BX) + round8(BX + mwlt - 1));
-    const size_t tab = (size_t)gram_tab_bytes(nrows), per = (size_t)nrows * kRowBytes;
-    if (tab + 2 * per > lim) continue;
-    p.BX = BX;
-    p.BXp = round8(BX);
-    p.nblk = (N0 + BX - 1) / BX;
-    p.NYB = BX + mwlt - 1;
-    p.NYBp = round8(p.NYB);
-    p.nrows = nrows;
-    p.stages = (int)std::min<size_t>(4, (lim - tab) / per);
-    if (tune->stages >= 2 && tune->stages < p.stages) p.stages = tune->stages;
-    p.smem = tab + (size_t)p.stages * per;
-    break;
+  // the (occupancy, order) groups in table order: the first is the level
+  // count's default, a later one serves where the default's rows do not fit
+  // its shared memory (two blocks per SM on a long time extent)
+  for (int grp = 0; grp < nc && p.BX == 0; grp++) {
+    bool seen = false;
+    for (int c = 0; c < grp; c++)
+      seen = seen || (cand[c].occ == cand[grp].occ && cand[c].ord == cand[grp].ord);
+    if (seen) continue;
+    // the group's variant with the extents per thread that waste the fewest
+    // (ties: the first listed)
+    int best = -1, bw = 1 << 30;
+    for (int c = grp; c < nc; c++) {
+      if (cand[c].occ != cand[grp].occ || cand[c].ord != cand[grp].ord) continue;
+      const int ng = (mwlt + cand[c].TQ - 1) / cand[c].TQ;
+      const int waste = ng * cand[c].TQ - mwlt;
+      if (waste < bw) {
+        bw = waste;
+        best = c;
+      }
+    }
+    const int TQ = cand[best].TQ, occ = cand[best].occ;
+    const int NG = (mwlt + TQ - 1) / TQ;
+    const int cap = gram_threads(occ);
+    if (NG > cap) continue;
+    const int bxmax = std::min(cap / NG, tune->bx > 0 ? tune->bx : N0);
+    // the fewest start-slice blocks whose rows fit two stages in the shared
+    // memory of one block (half an SM's for two blocks per SM)
+    const size_t lim = gram_blocks_per_sm(occ) == 2 ? 113 * 1024 : 227 * 1024;
+    for (int nblk = (N0 + bxmax - 1) / bxmax; nblk <= N0; nblk++) {
+      const int BX = (N0 + nblk - 1) / nblk;
+      const int nrows = msl * (round8(BX) + round8(BX + mwlt - 1));
+      const size_t tab = (size_t)gram_tab_bytes(nrows), per = (size_t)nrows * kRowBytes;
+      if (tab + 2 * per > lim) continue;
+      p.TQ = TQ;
+      p.occ = occ;
+      p.ord = cand[best].ord;
+      p.NG = NG;
+      p.BX = BX;
+      p.BXp = round8(BX);
+      p.nblk = (N0 + BX - 1) / BX;
+      p.NYB = BX + mwlt - 1;
+      p.NYBp = round8(p.NYB);
+      p.nrows = nrows;
+      p.stages = (int)std::min<size_t>(4, (lim - tab) / per);
+      if (tune->stages >= 2 && tune->stages < p.stages) p.stages = tune->stages;
+      p.smem = tab + (size_t)p.stages * per;
+      break;
+    }
   }
   if (p.BX == 0) return false;
   // row offsets are kept as 32-bit multiples of 16 bytes
