@@ -37,8 +37,10 @@ int num_sms() {
   if (dev < 0 || dev >= 64) dev = 0;
   if (cached[dev] == 0) {
     int n = 0;
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
       n = 148;
+      cudaGetLastError();  // no GPU (host-only planning): drop the failed query's error
+    }
     cached[dev] = n;
   }
   return cached[dev];
@@ -1175,9 +1177,7 @@ int wlg_gram_plan_shape(const int n[4], int bc, int msl, int mwlt, int precision
     t.cpc = tune[4];
   }
   GramPlan gp;
-  const bool ok = gram_plan(gp, make_geo(n), bc, msl, mwlt, precision == WLG_FP64, &t);
-  cudaGetLastError();  // a host without a GPU leaves the SM-count query's error behind
-  if (!ok) {
+  if (!gram_plan(gp, make_geo(n), bc, msl, mwlt, precision == WLG_FP64, &t)) {
     set_error("no temporal-gauge plan for msl %d, mwlt %d", msl, mwlt);
     return -1;
   }
