@@ -89,3 +89,14 @@ def test_c3_default_shapes():
         (1, 3, 32, 2, 3, 75, 738)
     p = plan((64, 32, 32, 32), 3, 6, 24, WLG_FP64)
     assert (p["occ"], p["tq"], p["bx"], p["nblk"], p["cpc"], p["nsplit"]) == (2, 1, 8, 8, 499, 222)
+
+
+def test_plans_refused():
+    """Level counts outside 1..8, a time extent whose extent groups exceed a
+    block, or an unknown precision give -1 and a message, not a plan."""
+    n = (64, 32, 32, 32)
+    for msl, mwlt, prec in ((0, 4, WLG_MIXED), (9, 4, WLG_FP64), (6, 0, WLG_MIXED),
+                            (6, 4000, WLG_MIXED), (6, 4000, WLG_FP64), (6, 4, 7)):
+        assert plan(n, 3, msl, mwlt, prec) is None, (msl, mwlt, prec)
+        assert lib.wlg_last_error()
+    assert plan(n, 3, 6, 24, WLG_MIXED) is not None
