@@ -28,7 +28,7 @@ static void init(void)
   }
 }
 
-/* lattice extents (N0..N3) of this build; returns its MAX_SM_LEVELS */
+/* lattice extents (N0..N3) of this library; returns its MAX_SM_LEVELS */
 int wlref_dims(int n[4])
 {
   n[0] = N0; n[1] = N1; n[2] = N2; n[3] = N3;
@@ -149,7 +149,7 @@ static void set_parms(int msl, const int *nss, int mwlt, int mwlr, int op_smear,
   int k, n[MAX_SM_LEVELS];
   double aa[3], ah[2];
   error(msl < 1 || msl > MAX_SM_LEVELS, 1, "set_parms [driver.c]",
-        "msl=%d is outside 1..MAX_SM_LEVELS of this build", msl);
+        "msl=%d is outside 1..MAX_SM_LEVELS of this library", msl);
   for (k = 0; k < msl; k++)
     n[k] = nss[k];
   aa[0] = alpha_action[0]; aa[1] = alpha_action[1]; aa[2] = alpha_action[2];

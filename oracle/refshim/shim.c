@@ -6,7 +6,7 @@
  * Geometry.  Sites are numbered as openQCD numbers them on one process: the
  * even points (x0+x1+x2+x3 even) first, then the odd points; ipt[] maps the
  * lexicographic index x3 + L3*x2 + L2*L3*x1 + L1*L2*L3*x0 to that number.
- * Within one parity this build keeps lexicographic order (openQCD orders
+ * Within one parity this shim keeps lexicographic order (openQCD orders
  * sites inside its blocks differently; that only changes the order of the
  * floating-point sums over sites).  iup/idn wrap periodically in every
  * direction, as openQCD's do when a direction has one process.
@@ -309,27 +309,27 @@ int fdigits(double x)
  * error of the driver */
 int find_section(char *title)
 {
-  error(1, 1, "find_section [shim.c]", "input files are not read in this build (%s)", title);
+  error(1, 1, "find_section [shim.c]", "input files are not read by this shim (%s)", title);
   return 0;
 }
 
 int read_line(char *tag, char *format, ...)
 {
   (void)format;
-  error(1, 1, "read_line [shim.c]", "input files are not read in this build (%s)", tag);
+  error(1, 1, "read_line [shim.c]", "input files are not read by this shim (%s)", tag);
   return 0;
 }
 
 void read_iprms(char *tag, int n, int *iprms)
 {
   (void)n; (void)iprms;
-  error(1, 1, "read_iprms [shim.c]", "input files are not read in this build (%s)", tag);
+  error(1, 1, "read_iprms [shim.c]", "input files are not read by this shim (%s)", tag);
 }
 
 void read_dprms(char *tag, int n, double *dprms)
 {
   (void)n; (void)dprms;
-  error(1, 1, "read_dprms [shim.c]", "input files are not read in this build (%s)", tag);
+  error(1, 1, "read_dprms [shim.c]", "input files are not read by this shim (%s)", tag);
 }
 
 /* ---- MPI on one rank ----------------------------------------------------- */

@@ -117,7 +117,7 @@ typedef struct {
     _wlref_col(wlref_p_,w,2); _su3_multiply(wlref_q_,v,wlref_p_); _wlref_setcol(u,2,wlref_q_); \
     _wlref_col(wlref_p_,w,3); _su3_multiply(wlref_q_,v,wlref_p_); _wlref_setcol(u,3,wlref_q_); }
 
-/* the SSE prefetch hint is a no-op in this build (SSE2 is not defined) */
+/* the SSE prefetch hint is a no-op here (SSE2 is not defined) */
 #define _prefetch_su3_dble(addr)
 
 /* ---- su3fcts.h: out-of-line products (w may be the same matrix as v) --- */

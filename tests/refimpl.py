@@ -101,7 +101,7 @@ class Ref:
 
     def _loops(self, fn, p):
         if p.msl > self.max_levels:
-            raise ValueError(f"msl {p.msl} > MAX_SM_LEVELS {self.max_levels} of this build")
+            raise ValueError(f"msl {p.msl} > MAX_SM_LEVELS {self.max_levels} of this library")
         wl = np.empty(p.msl * p.msl * p.mwlt * p.mwlr * self.n[0])
         nss = (C.c_int * p.msl)(*[int(x) for x in p.nss[:p.msl]])
         aa = (C.c_double * 3)(*p.alpha_action)
