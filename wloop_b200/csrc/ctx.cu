@@ -384,6 +384,21 @@ static int do_smear(wlg_ctx* c, const wlg_wloop_parms* p, double* plaq) {
 // reduction.  Returns 1 (nothing done) when the form does not apply: shapes
 // that do not fit, or a gauge field too far from unitary (links smeared
 // without projection), which the other forms then measure.
+// The smearing and upload scratch (HYP levels, APE ping-pong, spatial-HYP
+// level, host staging) is idle during the loop stage and allocated again by
+// the next measurement that needs it: it is returned to the device when the
+// loop stage's buffers do not fit beside it (FP64 at 48^3x96 holds 58 GB of
+// it).  cudaFree waits for the device, so no copy or kernel still uses it.
+static void release_idle_scratch(wlg_ctx* c) {
+  release(c->bar);
+  release(c->til);
+  release(c->apeA);
+  release(c->apeB);
+  release(c->dl);
+  release(c->staging);
+  set_error("%s", "");
+}
+
 template <class T>
 static int do_loops_gram(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
   typedef typename V2<T>::t T2;
@@ -412,9 +427,23 @@ static int do_loops_gram(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
     memcpy(&dev, &bits, sizeof(dev));
   }
   if (!(dev <= kGramMaxDeviation)) return 1;
-  if (ensure(c->gUh, nb) || ensure(c->gB, nb) || ensure(c->gA, na) ||
-      ensure(c->partial, gp.partial_elems * sizeof(T)) || ensure(c->wl, sizeof(double) * nwl))
-    return -1;
+  auto alloc = [&]() {
+    return ensure(c->gUh, nb) || ensure(c->gB, nb) || ensure(c->gA, na) ||
+           ensure(c->partial, gp.partial_elems * sizeof(T)) || ensure(c->wl, sizeof(double) * nwl);
+  };
+  if (alloc()) {
+    release_idle_scratch(c);
+    if (alloc()) {
+      // no room for the transformed lines: the carried-line form measures
+      set_error("%s", "");
+      release(c->gUh);
+      release(c->gB);
+      release(c->gA);
+      release(c->gG);
+      release(c->gH);
+      return 1;
+    }
+  }
   c->used_variant = 11;
   c->lines_len = 0;
   c->lines_at = nullptr;
@@ -482,13 +511,18 @@ static int do_loops(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
   c->lines_lazy = 0;
   c->used_variant = cp.variant;
   size_t nwl = (size_t)msl * msl * p->mwlt * p->mwlr * g.n[0];
-  if (ensure(c->partial, sizeof(double) * cp.partial_doubles) || ensure(c->wl, sizeof(double) * nwl))
-    return -1;
-  if (p->mwlr > 1 && ensure(c->lines, f3 * msl)) return -1;
   // forms 4 and 5 compute the lines of the next R inside the contraction
   // (ping-pong between two line buffers); other forms run the line step
   const bool fuse = contract_fuses_lines(cp);
-  if (fuse && p->mwlr > 2 && ensure(c->lines2, f3 * msl)) return -1;
+  auto alloc = [&]() {
+    return ensure(c->partial, sizeof(double) * cp.partial_doubles) ||
+           ensure(c->wl, sizeof(double) * nwl) || (p->mwlr > 1 && ensure(c->lines, f3 * msl)) ||
+           (fuse && p->mwlr > 2 && ensure(c->lines2, f3 * msl));
+  };
+  if (alloc()) {
+    release_idle_scratch(c);
+    if (alloc()) return -1;
+  }
   c->lines_len = 0;
   c->lines_at = nullptr;
   const T2* lev = (const T2*)c->levels.p;
