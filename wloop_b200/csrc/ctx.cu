@@ -379,11 +379,6 @@ static int do_smear(wlg_ctx* c, const wlg_wloop_parms* p, double* plaq) {
   return 0;
 }
 
-// wloops() in the temporal gauge (gram.cu): the gauge field and H^-1 once,
-// then the first lines; per R the line step, the banded Gram product and its
-// reduction.  Returns 1 (nothing done) when the form does not apply: shapes
-// that do not fit, or a gauge field too far from unitary (links smeared
-// without projection), which the other forms then measure.
 // The smearing and upload scratch (HYP levels, APE ping-pong, spatial-HYP
 // level, host staging) is idle during the loop stage and allocated again by
 // the next measurement that needs it: it is returned to the device when the
@@ -399,6 +394,11 @@ static void release_idle_scratch(wlg_ctx* c) {
   set_error("%s", "");
 }
 
+// wloops() in the temporal gauge (gram.cu): the gauge field and H^-1 once,
+// then the first lines; per R the line step, the banded Gram product and its
+// reduction.  Returns 1 (nothing done) when the form does not apply: shapes
+// that do not fit, or a gauge field too far from unitary (links smeared
+// without projection), which the other forms then measure.
 template <class T>
 static int do_loops_gram(wlg_ctx* c, const wlg_wloop_parms* p, double* wl_mat) {
   typedef typename V2<T>::t T2;
