@@ -23,7 +23,10 @@ from tests import oracle as O
 from wloop_b200.api import APE, HYP, WloopParms
 
 
-def temporal_gauge_wloops(n, bc, u, levels, p):
+def transformed_lines(n, bc, u, levels, p):
+    """Per spatial extent R = 1..mwlr: (R, VA, VB), the A lines of the N0
+    start slices and the B lines of the Nu unrolled slices as rows
+    [slice][level][column], column = (direction, site, 18 reals)."""
     N0 = n[0]
     ns = np.array(n[1:])
     vs = int(np.prod(ns))
@@ -50,8 +53,6 @@ def temporal_gauge_wloops(n, bc, u, levels, p):
     for k in range(3):
         b[:, k] = g[None] @ lev[:, :, :, k] @ dag(g[:, shifted(k, 1)])[None]
         uh[:, k] = hinv[None] @ b[:, k]
-    norm = 9.0 * vs
-    wl = np.zeros(N0 * mwlr * mwlt * msl * msl)
     a = np.empty((msl, 3, N0, vs, 3, 3), dtype=np.complex128)
 
     def rows(m, ny):
@@ -64,16 +65,31 @@ def temporal_gauge_wloops(n, bc, u, levels, p):
             if r > 0:
                 b[:, k] = b[:, k] @ uh[:, k][:, :, shifted(k, r)]
             a[:, k] = hinv[None, :N0] @ b[:, k, :N0] @ hinv[None, :N0][:, :, shifted(k, R)]
-        va, vb = rows(a, N0), rows(b, Nu)
+        yield R, rows(a, N0), rows(b, Nu)
+
+
+def banded_gram(n, bc, p, lines, dot=lambda va, vb: va @ vb.T):
+    """wl_mat (wl_idx order) from the transformed lines: W(x0, T) =
+    dot(VA[x0], VB[x0 + T]) / (9 N1 N2 N3); loops through the last slice of
+    open time are exact zeros."""
+    N0, msl, mwlt, mwlr = n[0], p.msl, p.mwlt, p.mwlr
+    norm = 9.0 * n[1] * n[2] * n[3]
+    wl = np.zeros(N0 * mwlr * mwlt * msl * msl)
+    for R, va, vb in lines:
+        r = R - 1
         for x0 in range(N0):
             for T in range(1, mwlt + 1):
                 if bc == 0 and x0 + T >= N0:
                     continue  # through the zero temporal link of the last slice
-                w = va[x0] @ vb[x0 + T].T / norm  # [s1][s2]
+                w = dot(va[x0], vb[x0 + T]) / norm  # [s1][s2]
                 for s1 in range(msl):
                     for s2 in range(msl):
                         wl[s1 + msl * (s2 + msl * (T - 1 + mwlt * (r + mwlr * x0)))] = w[s1, s2]
     return wl
+
+
+def temporal_gauge_wloops(n, bc, u, levels, p):
+    return banded_gram(n, bc, p, transformed_lines(n, bc, u, levels, p))
 
 
 CASES = [
