@@ -309,7 +309,9 @@ int wlg_gram_shape(wlg_ctx* ctx, int msl, int mwlt, int* shape);
  * {extents per thread, occ, ord, start slices per block, its rows padded to
  * 8, extent groups, B rows per level, padded to 8, blocks of start slices,
  * staged rows, stages, threads per block, shared memory bytes per block,
- * column chunks, chunks per block, column splits}. */
+ * column chunks, chunks per block, column splits}.  Lattices and boundary
+ * conditions that wlg_create refuses are refused here too; -1 also when no
+ * plan fits (the carried-line form then measures). */
 int wlg_gram_plan_shape(const int n[4], int bc, int msl, int mwlt, int precision,
                         const int tune[5], long long shape[16]);
 /* The context's CUDA stream (cudaStream_t), for callers that record events. */

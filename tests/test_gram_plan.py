@@ -100,3 +100,8 @@ def test_plans_refused():
         assert plan(n, 3, msl, mwlt, prec) is None, (msl, mwlt, prec)
         assert lib.wlg_last_error()
     assert plan(n, 3, 6, 24, WLG_MIXED) is not None
+    # lattices and boundary conditions a context refuses
+    for bad, bc in (((0, 4, 4, 4), 3), ((8, 1, 4, 4), 3), ((-8, 4, 4, 4), 0),
+                    ((2048, 1024, 1024, 2), 3), ((8, 4, 4, 4), 1)):
+        assert plan(bad, bc, 2, 2, WLG_MIXED) is None, bad
+        assert lib.wlg_last_error()

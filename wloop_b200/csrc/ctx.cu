@@ -1198,8 +1198,19 @@ int wlg_gram_shape(wlg_ctx* c, int msl, int mwlt, int* shape) {
 int wlg_gram_plan_shape(const int n[4], int bc, int msl, int mwlt, int precision,
                         const int tune[5], long long shape[16]) {
   set_error("%s", "");
-  if (!n || !shape || (precision != WLG_FP64 && precision != WLG_MIXED)) {
+  if (!n || !shape || (precision != WLG_FP64 && precision != WLG_MIXED) ||
+      (bc != 0 && bc != 3)) {
     set_error("gram_plan_shape: bad arguments");
+    return -1;
+  }
+  // the lattices wlg_create accepts
+  for (int i = 0; i < 4; i++)
+    if (n[i] < 2) {
+      set_error("gram_plan_shape: lattice extent N%d=%d < 2", i, n[i]);
+      return -1;
+    }
+  if ((long long)n[0] * n[1] * n[2] * n[3] > (1LL << 30)) {
+    set_error("gram_plan_shape: lattice volume too large");
     return -1;
   }
   GramTuning t;
