@@ -105,3 +105,17 @@ def test_plans_refused():
                     ((2048, 1024, 1024, 2), 3), ((8, 4, 4, 4), 1)):
         assert plan(bad, bc, 2, 2, WLG_MIXED) is None, bad
         assert lib.wlg_last_error()
+
+
+def test_batch_estimate_refuses_bad_lattices():
+    """The batch memory estimate (host only, used by the serving loop's
+    admission) refuses what wlg_batch_create refuses, instead of planning a
+    lattice with a zero extent."""
+    from wloop_b200 import APE, WloopParms
+    from wloop_b200.api import estimate_bytes
+    p = WloopParms(msl=2, nss=[0, 1], mwlt=1, mwlr=1, op_smear=APE, alpha_ape=0.5, proj_iter=4)
+    assert estimate_bytes((8, 4, 4, 4), 3, p, "mixed") > 0
+    assert estimate_bytes((64, 32, 32, 32), 3, p, "fp64") > estimate_bytes((64, 32, 32, 32), 3, p)
+    for n, bc in (((0, 4, 4, 4), 3), ((8, 0, 4, 4), 3), ((8, 4, 4, 4), 1),
+                  ((2048, 1024, 1024, 2), 3)):
+        assert estimate_bytes(n, bc, p, "mixed") == -1, (n, bc)

@@ -167,6 +167,15 @@ template <class T> Links<T> lview(char* base, size_t D, int ndir, int first_mu) 
   return L;
 }
 
+// the lattices a context accepts (wlg_create): extents of at least 2, at
+// most 2^30 sites, open or periodic time; 0 or -1
+static int check_lattice(const int* n, int bc) {
+  for (int i = 0; i < 4; i++)
+    if (n[i] < 2) return -1;
+  if ((long long)n[0] * n[1] * n[2] * n[3] > (1LL << 30)) return -1;
+  return (bc == 0 || bc == 3) ? 0 : -1;
+}
+
 int check_parms(const Geo& g, const wlg_wloop_parms& p) {
   if (p.msl < 1 || p.msl > WLG_MAX_SM_LEVELS) return -1;
   if (p.mwlt < 1 || p.mwlt > g.n[0] / 2 + 1) return -1;
@@ -827,16 +836,16 @@ int wlg_batch_create(int nconf, const int* dims, const int* bcs, const wlg_wloop
   for (int c = 0; c < nconf; c++) {
     Cfg f;
     memset(&f, 0, sizeof(f));
-    for (int i = 0; i < 4; i++)
-      if (dims[4 * c + i] < 2) {
-        set_error("batch_create: lattice %d has an extent < 2", c);
-        delete b;
-        return -1;
-      }
+    if (check_lattice(dims + 4 * c, bcs[c])) {
+      set_error("batch_create: lattice %d: an extent < 2, more than 2^30 sites, or a boundary "
+                "condition other than 0 and 3", c);
+      delete b;
+      return -1;
+    }
     f.g = make_geo(dims + 4 * c);
     f.bc = bcs[c];
     f.p = parms[c];
-    if ((f.bc != 0 && f.bc != 3) || check_parms(f.g, f.p)) {
+    if (check_parms(f.g, f.p)) {
       set_error("batch_create: configuration %d: bad boundary condition or parameters", c);
       delete b;
       return -1;
@@ -1059,11 +1068,13 @@ int wlg_batch_use_graph(wlg_batch* b, int on) {
 long long wlg_batch_estimate_bytes(int nconf, const int* dims, const int* bcs,
                                    const wlg_wloop_parms* parms, int precision) {
   if (nconf < 1 || !dims || !bcs || !parms) return -1;
+  if (precision != WLG_FP64 && precision != WLG_MIXED) return -1;
   wlg_batch tmp;
   tmp.prec = precision;
   for (int c = 0; c < nconf; c++) {
     Cfg f;
     memset(&f, 0, sizeof(f));
+    if (check_lattice(dims + 4 * c, bcs[c])) return -1;
     f.g = make_geo(dims + 4 * c);
     f.bc = bcs[c];
     f.p = parms[c];

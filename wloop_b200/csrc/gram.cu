@@ -613,7 +613,7 @@ bool gram_plan(GramPlan& p, const Geo& g, int bc, int msl, int mwlt, bool fp64,
   GramTuning none;
   if (!tune) tune = &none;
   p = GramPlan();
-  if (msl < 1 || msl > 8 || mwlt < 1) return false;
+  if (msl < 1 || msl > 8 || mwlt < 1 || g.n[0] < 1 || g.vs < 1) return false;
   const int esz = fp64 ? 8 : 4;
   p.esize = esz;
   p.L = msl;
