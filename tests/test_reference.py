@@ -150,6 +150,24 @@ def test_oracle_measurement_matches_reference(case):
     assert np.abs(ref.get_field() - uh).max() < 1e-13
 
 
+# 131,072 sites: above the size from which a context measures in the
+# temporal gauge by default
+LARGE = [((32, 16, 16, 16), bc, WloopParms(msl=3, nss=[0, 2, 2], mwlt=3, mwlr=2, op_smear=APE,
+                                           alpha_ape=0.5, proj_iter=4)) for bc in (3, 0)]
+
+
+@pytest.mark.parametrize("case", range(len(LARGE)))
+def test_oracle_matches_reference_on_a_large_lattice(case):
+    n, bc, p = LARGE[case]
+    ref = need(n)
+    u = O.generate_links(n, bc, 300 + case, 0.25)
+    ref.set_field(bc, u)
+    got = ref.measure(p)
+    uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
+    want, want_abs = O.wloop_sum(n, bc, uh, p, want_abs=True)
+    assert scaled_err(got, want, want_abs) <= 1e-13
+
+
 def test_reference_reproduces_c1_fixture():
     """The 8^4 workload's golden fixture (made by the oracle) reproduced by
     the reference itself."""
@@ -203,6 +221,34 @@ def test_gpu_matches_reference(case, form):
     relm = np.abs(gm - want)[nz] / np.abs(want)[nz]
     print(f"mixed vs reference: max plain relative {relm.max():.2e}")
     assert relm.max() <= 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", range(len(LARGE)))
+def test_gpu_default_form_matches_reference_on_a_large_lattice(case):
+    """32x16^3 (131,072 sites): a context's default there is the temporal
+    gauge form; against the reference itself, both precisions."""
+    from wloop_b200 import Context
+    n, bc, p = LARGE[case]
+    ref = need(n)
+    u = O.generate_links(n, bc, 400 + case, 0.25)
+    ref.set_field(bc, u)
+    want = ref.measure(p)
+    uh = O.hyp_links(n, bc, u, *p.alpha_action, p.proj, p.proj_iter)
+    _, want_abs = O.wloop_sum(n, bc, uh, p, want_abs=True)
+    nz = want != 0.0
+    for prec in ("fp64", "mixed"):
+        with Context(n, bc, prec) as c:
+            c.upload(u)
+            got = c.measure(p)
+            assert c.contract_form == 11
+        assert np.all(got[~nz] == 0.0)
+        rel = np.abs(got - want)[nz] / np.abs(want)[nz]
+        print(f"{prec} vs reference: max plain relative {rel.max():.2e}")
+        if prec == "fp64":
+            assert scaled_err(got, want, want_abs) <= 1e-12
+        else:
+            assert rel.max() <= 1e-6
 
 
 @pytest.mark.gpu
